@@ -1,0 +1,280 @@
+/*
+ * efsi.h — C ABI of the B200 implementation of EulerianFSI.jl's four-stage
+ * IMEX fractional step (`integrate_step!`).
+ *
+ * The library owns every device buffer of one simulation context behind an
+ * opaque handle.  Host arrays are Julia-style column-major (x index fastest)
+ * FP64 matrices:
+ *   U            (Nx+1) x Ny      x-face velocity
+ *   V            Nx x (Ny+1)      y-face velocity
+ *   cell fields  Nx x Ny          phi, resource c, sigma_xx, sigma_yy, sigma_xy,
+ *                                 growth target G, correction potential q
+ * Host pointers are only read or written during a call and never retained.
+ * Every call is synchronous: results are valid on return.  One handle must not
+ * be used by two host threads at the same time.
+ *
+ * Every entry point returns an EFSI_* status.  Non-zero statuses map onto the
+ * exception types the reference throws (see the EFSI_* list below); the message
+ * text is available from efsi_last_error().
+ */
+#ifndef EFSI_H
+#define EFSI_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EFSI_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------- */
+#define EFSI_OK            0
+#define EFSI_ARG           1  /* Julia ArgumentError (e.g. TimeIntegrationIMEX.jl:1121, Projection.jl:213) */
+#define EFSI_DIM           2  /* Julia DimensionMismatch (TimeIntegrationIMEX.jl:500-516)                    */
+#define EFSI_SOLVE         3  /* Julia ErrorException from a linear solve (Projection.jl:281, :293)          */
+#define EFSI_DOMAIN        4  /* Julia DomainError, non-SPD structure tensor (StructureTensor.jl:491-496)     */
+#define EFSI_CUDA          5  /* CUDA runtime failure or no usable device                                    */
+#define EFSI_UNSUPPORTED   6  /* valid reference input that the device step does not implement              */
+
+/* ---- boundary conditions (BoundaryConditions.jl:23-46) ------------------- */
+#define EFSI_BC_PERIODIC           0
+#define EFSI_BC_DIRICHLET          1
+#define EFSI_BC_NEUMANN            2
+#define EFSI_BC_MIXED              3
+#define EFSI_BC_ADVECTIVE_OUTFLOW  4
+
+/* One side of a BoundaryConditionSetup.  Julia boundary data may be a scalar,
+ * a vector or a callable (BoundaryConditions.jl:103-136); the host flattens all
+ * three into `value[0..n)`, indexed by the reference's 1-based boundary index
+ * minus one.  Required lengths per side (left/right, bottom/top):
+ *   U: Ny, Nx+1      V: Ny+1, Nx      cell-centred fields: Ny, Nx            */
+typedef struct efsi_bc_side {
+    int32_t        type;      /* EFSI_BC_*                                              */
+    int32_t        n;         /* entries in value / neumann / mask                      */
+    const double*  value;     /* Dirichlet or Neumann datum; MIXED Dirichlet datum;
+                                 ADVECTIVE_OUTFLOW backflow datum                       */
+    const double*  neumann;   /* MIXED only: Neumann datum                              */
+    const uint8_t* mask;      /* MIXED only: 1 where the point is Dirichlet             */
+} efsi_bc_side;
+
+typedef struct efsi_bc_setup {
+    efsi_bc_side left, right, bottom, top;
+} efsi_bc_setup;
+
+/* MeshMetrics (MeshGeneration.jl:41-73).  The device step requires uniform
+ * spacing in each direction (every configuration of the benchmark suite is
+ * uniform); stretched metrics are rejected with EFSI_UNSUPPORTED. */
+typedef struct efsi_mesh {
+    int32_t Nx, Ny;
+    double  Lx, Ly;
+    int32_t periodic_x, periodic_y;
+    const double *dx_f, *dx_c, *dy_f, *dy_c;                 /* Nx+1, Nx, Ny+1, Ny */
+    const double *wL_c2fx, *wR_c2fx, *wB_c2fy, *wT_c2fy;     /* Nx+1, Nx+1, Ny+1, Ny+1 */
+    const double *wL_f2cx, *wR_f2cx, *wB_f2cy, *wT_f2cy;     /* Nx, Nx, Ny, Ny */
+    const double *dx_west_corner, *dx_east_corner;           /* Nx+1 */
+    const double *dy_south_corner, *dy_north_corner;         /* Ny+1 */
+} efsi_mesh;
+
+/* ---- model selections (FSIModels, TimeIntegrationIMEX.jl:156-208) -------- */
+#define EFSI_GROWTH_NONE            0   /* NoGrowth                          GrowthModels.jl:51   */
+#define EFSI_GROWTH_CONSTANT        1   /* ConstantIntrinsicGrowth(rate)     GrowthModels.jl:67   */
+#define EFSI_GROWTH_SATURATING      2   /* SaturatingResourceGrowth(rate,K)  GrowthModels.jl:90   */
+
+#define EFSI_GTENSOR_ISOTROPIC      0   /* IsotropicGrowthTensor             GrowthModels.jl:126  */
+#define EFSI_GTENSOR_DIRECTIONAL    1   /* DirectionalGrowthTensor(tx,ty)    GrowthModels.jl:150  */
+
+#define EFSI_VISC_NONE              0   /* NoViscosity                 TransportConstitutive.jl:82  */
+#define EFSI_VISC_CONSTANT          1   /* ConstantViscosity           TransportConstitutive.jl:89  */
+#define EFSI_VISC_HARMONIC          2   /* HarmonicPhaseViscosity      TransportConstitutive.jl:115 */
+
+#define EFSI_DIFF_NONE              0   /* NoDiffusion                 TransportConstitutive.jl:175 */
+#define EFSI_DIFF_CONSTANT          1   /* ConstantDiffusivity         TransportConstitutive.jl:178 */
+#define EFSI_DIFF_HARMONIC          2   /* HarmonicPhaseDiffusivity    TransportConstitutive.jl:201 */
+
+#define EFSI_CONSUMPTION_NONE       0   /* NoResourceConsumption          TransportConstitutive.jl:250 */
+#define EFSI_CONSUMPTION_SATURATING 1   /* SaturatingResourceConsumption  TransportConstitutive.jl:264 */
+
+#define EFSI_RELAX_NONE             0   /* NoRelaxation           StructuralConstitutive.jl:19 */
+#define EFSI_RELAX_MAXWELL          1   /* MaxwellRelaxation      StructuralConstitutive.jl:22 */
+
+#define EFSI_ELASTIC_NONE           0   /* NoElasticStress             StructuralConstitutive.jl:38 */
+#define EFSI_ELASTIC_LINEAR         1   /* LinearInternalTensorStress  StructuralConstitutive.jl:40 */
+
+#define EFSI_CAP_NONE               0   /* NoCapillarity                                  */
+#define EFSI_CAP_DIFFUSE_AREA       1   /* DiffuseAreaCapillarity     Capillarity.jl:21   */
+
+/* phase_field_method; parameters in pf_param[] / pf_option:
+ *   UPWIND : NoPhaseFieldRegularization, or LegacySplit(NoInterfaceFlux)    PhaseFieldMethods.jl:33
+ *   CDI    : CurrentCDIPhaseField / LegacySplit(ConservativeDiffuseInterfaceFlux)
+ *            pf_param = {inverse_peclet, epsilon, delta_normal}             InterfaceRegularization.jl:23
+ *   ACDI   : JainACDIPhaseField; pf_param = {gamma, epsilon, psi_floor, delta_normal},
+ *            pf_option = dynamic_gamma                                      PhaseFieldMethods.jl:54
+ *   UWCDI  : PirozzoliUWCDIPhaseField; pf_param = {alpha, delta_normal},
+ *            pf_option = EFSI_NORMALS_*                                     PhaseFieldMethods.jl:97 */
+#define EFSI_PF_UPWIND              0
+#define EFSI_PF_CDI                 1
+#define EFSI_PF_ACDI                2
+#define EFSI_PF_UWCDI               3
+#define EFSI_NORMALS_STANDARD       0
+#define EFSI_NORMALS_YOUNGS         1
+#define EFSI_NORMALS_SMOOTHED9      2
+
+#define EFSI_FORCE_NONE             0   /* NoBodyForce                                        */
+#define EFSI_FORCE_CONSTANT         1   /* ConstantBodyForce(fx,fy)   TransportConstitutive.jl:318 */
+#define EFSI_FORCE_KOLMOGOROV       2   /* KolmogorovBodyForce(A,k;phase) TransportConstitutive.jl:340 */
+
+typedef struct efsi_models {
+    int32_t growth_source;        double growth_rate, growth_half_saturation;
+    int32_t growth_tensor;        double growth_direction_x, growth_direction_y;
+    int32_t viscosity;            double viscosity_fluid, viscosity_structure;
+    int32_t diffusivity;          double diffusivity_fluid, diffusivity_structure;
+    int32_t resource_consumption; double consumption_rate, consumption_half_saturation;
+    int32_t tensor_relaxation;    double relaxation_rate;
+    int32_t elastic_stress;       double elastic_coefficient;
+    int32_t capillarity;          double capillary_coefficient, capillary_delta_normal;
+    int32_t capillary_smoothing_passes;
+    int32_t phase_field_method;   double pf_param[4];   int32_t pf_option;
+    int32_t body_force;           double body_force_param[3];  /* (fx,fy,-) or (A,k,phase) */
+} efsi_models;
+
+/* ---- numerics (IMEXNumerics + LinearSolverOptions, TimeIntegrationIMEX.jl:211-301) */
+#define EFSI_EXT_NONE               0   /* NoStructureExtension         StructureTensor.jl:63  */
+#define EFSI_EXT_IDENTITY_OUTSIDE   1   /* IdentityOutsideStructure     StructureTensor.jl:73  */
+#define EFSI_EXT_GEOMETRIC          2   /* GeometricStructureExtension  StructureTensor.jl:106 */
+
+#define EFSI_PRECISION_FP64         0   /* plain FP64 step                                        */
+#define EFSI_PRECISION_MIXED        1   /* FP32 stencil bulk and multigrid, FP64 state, residuals,
+                                           inner products, refinement and mass sums               */
+
+typedef struct efsi_numerics {
+    int32_t structure_extension;  double extension_rate, extension_exponent, extension_cutoff;
+    double  projection_reltol;    int32_t projection_maxiter;
+    double  stage1_constraint_atol, stage1_constraint_rtol;
+    int32_t check_stage1_constraint;
+    double  linear_reltol;        int32_t linear_maxiter;    /* velocity and resource solves */
+    int32_t precision;            /* EFSI_PRECISION_*                                          */
+    int32_t reserved[7];
+} efsi_numerics;
+
+typedef struct efsi_config {
+    int32_t       abi_version;    /* EFSI_ABI_VERSION */
+    efsi_mesh     mesh;
+    efsi_bc_setup bc_U, bc_V, bc_correction, bc_phi, bc_resource;
+    efsi_bc_setup bc_sigma_xx, bc_sigma_yy, bc_sigma_xy;
+    efsi_models   models;
+    efsi_numerics numerics;
+} efsi_config;
+
+/* StepReport (TimeIntegrationIMEX.jl:318-327). */
+typedef struct efsi_step_report {
+    double  maximum_projection_constraint_linf;
+    double  maximum_growth_trace_error;
+    double  minimum_phi;
+    double  maximum_phi;
+    double  minimum_resource;
+    double  minimum_sigma_eigenvalue;
+    double  maximum_abs_sigma_determinant_error;
+    int64_t non_spd_cells;
+} efsi_step_report;
+
+/* ProjectionResult (Projection.jl:31-37) without the correction matrix, which is
+ * read with efsi_get_correction(). */
+typedef struct efsi_projection_result {
+    double linear_relative_residual;
+    double constraint_linf;
+    double constraint_l2;
+    double compatibility_defect;
+} efsi_projection_result;
+
+/* Solver statistics of the most recent step or projection. */
+typedef struct efsi_stats {
+    int32_t projection_iterations[4];   /* per stage; [0] = make_velocity_compatible      */
+    int32_t velocity_iterations[4];     /* per stage (stages 2..4)                        */
+    int32_t resource_iterations[4];
+    int64_t kernel_launches;            /* kernels enqueued by the last call              */
+} efsi_stats;
+
+typedef struct efsi_handle efsi_handle;
+
+/* build_imex_context + allocate_imex_workspace (TimeIntegrationIMEX.jl:468-493,
+ * :389-441): validates the configuration (periodicity agreement, :447-466;
+ * supported viscous boundaries, Operators.jl:89-105), uploads boundary data and
+ * allocates every device buffer on the current CUDA device.  On failure *out is
+ * NULL and efsi_last_error(NULL) describes the cause. */
+int  efsi_create(const efsi_config* config, efsi_handle** out);
+void efsi_destroy(efsi_handle* handle);
+/* Message of the last failing call on `handle` (NULL: last failing efsi_create
+ * on this thread). */
+const char* efsi_last_error(const efsi_handle* handle);
+
+/* Copy a full FSIState (TimeIntegrationIMEX.jl:103-118) to / from the device. */
+int efsi_upload_state(efsi_handle* h, const double* U, const double* V, const double* phi,
+                      const double* resource, const double* sigma_xx,
+                      const double* sigma_yy, const double* sigma_xy);
+int efsi_download_state(efsi_handle* h, double* U, double* V, double* phi, double* resource,
+                        double* sigma_xx, double* sigma_yy, double* sigma_xy);
+
+/* IMEXWorkspace.correction, the projection warm start (TimeIntegrationIMEX.jl:386). */
+int efsi_set_correction(efsi_handle* h, const double* q);
+int efsi_get_correction(efsi_handle* h, double* q);
+
+/* make_velocity_compatible! (TimeIntegrationIMEX.jl:1088-1109) on the device state. */
+int efsi_make_velocity_compatible(efsi_handle* h, efsi_projection_result* result);
+
+/* integrate_step! (TimeIntegrationIMEX.jl:1152-1256) on the device-resident state. */
+int efsi_integrate_step(efsi_handle* h, double t, double dt, efsi_step_report* report);
+
+/* integrate_step! as the drop-in sees it: the host FSIState arrays are uploaded,
+ * advanced in place and downloaded (TimeIntegrationIMEX.jl:1152-1256, with the
+ * state copies of :1169 and :1232-1238 crossing the host/device boundary). */
+int efsi_integrate_step_host(efsi_handle* h, double* U, double* V, double* phi,
+                             double* resource, double* sigma_xx, double* sigma_yy,
+                             double* sigma_xy, double t, double dt,
+                             efsi_step_report* report);
+
+/* n consecutive integrate_step! calls on the device-resident state with host
+ * sync only at the end; t advances by dts[k].  reports may be NULL or hold n
+ * entries.  On an error the state holds the last completed step and the
+ * return value says which step failed (efsi_last_error). */
+int efsi_step_n(efsi_handle* h, double t0, const double* dts, int32_t n,
+                efsi_step_report* reports);
+
+/* Projection.project! (Projection.jl:170-307) of host velocity arrays onto
+ * div(v) = target, using the context's correction boundaries and warm start. */
+int efsi_project(efsi_handle* h, double* U, double* V, const double* target,
+                 efsi_projection_result* result);
+
+/* phase_field_rhs for the context's phase-field method (PhaseFieldMethods.jl:408-475,
+ * :652-671, :852-867) with target divergence G. */
+int efsi_phase_field_rhs(efsi_handle* h, const double* U, const double* V, const double* phi,
+                         const double* G, double* rhs);
+
+/* structure_tensor_rhs (StructureTensor.jl:377-463) with K_g built from G by the
+ * context's growth-tensor model and the context's relaxation/extension. */
+int efsi_structure_tensor_rhs(efsi_handle* h, const double* sigma_xx, const double* sigma_yy,
+                              const double* sigma_xy, const double* U, const double* V,
+                              const double* phi, const double* G,
+                              double* rhs_xx, double* rhs_yy, double* rhs_xy);
+
+/* Explicit momentum forcing of one stage (TimeIntegrationIMEX.jl:959-985):
+ * -material_convection + body force + capillary force + div(phi tau_e)
+ * + growth-viscous force, on the full MAC faces. */
+int efsi_momentum_explicit_rhs(efsi_handle* h, double t, const double* U, const double* V,
+                               const double* phi, const double* sigma_xx,
+                               const double* sigma_yy, const double* sigma_xy,
+                               const double* G, double* Fx, double* Fy);
+
+/* apply_operator(build_viscous_operator(...), uv) (Operators.jl:929-1083, :1115)
+ * on the compact velocity vector uv = [U(1:Nx,:); V(:,1:Ny)] with viscosity
+ * evaluated from phi. */
+int efsi_apply_viscous_operator(efsi_handle* h, const double* phi, const double* uv,
+                                double* out);
+
+int efsi_get_stats(const efsi_handle* h, efsi_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EFSI_H */
