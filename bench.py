@@ -1,0 +1,289 @@
+"""Benchmark of the B200 IMEX fractional step (grid-cell-steps/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the 20-disk lid-driven cavity at 1024x1024 (ACDI, FP64, dt = 0.2 h), seeded
+synthetic initial fields.  A step is one integrate_step! of that grid.  `value` is
+timed with CUDA events on the library's stream around K device-resident steps
+(inputs already in HBM); `e2e` repeats the measurement through the public API
+(integrate_step with pinned host arrays, host<->device copies inside the timed
+region).  The working set (~0.5 GB) exceeds the 126 MB L2 on every step, so no
+extra L2 flush is inserted.  Multi-GPU runs are independent replicas (the step is a
+global elliptic solve and does not shard); rank 0 prints the aggregate.
+
+`--impl reference` times the FP64 CPU restatement of the reference step (the
+oracle; the Julia reference cannot run here) on the host cores for a bounded
+sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "grid-cell-steps/s"
+UNIT = "cell-steps/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                clk = float(parts[1])
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            sm.append(clk)
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        busy = [s for s in sm if s > 600] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_workload(args, precision):
+    from eulerianfsi_b200 import workloads
+    return workloads.cavity_disks20(N=args.N, steps=args.steps, projection_reltol=args.projection_reltol,
+                                    velocity_reltol=args.velocity_reltol, precision=precision)
+
+
+def cpu_sample(args, budget_s, max_steps):
+    """Time the FP64 CPU oracle (single thread) on the same workload."""
+    from oracle.oracle import Oracle
+    w = build_workload(args, "fp64")
+    o = Oracle(w.metrics, w.bcs, w.models, w.numerics)
+    o.upload(w.state)
+    done, t = 0, 0.0
+    start = time.perf_counter()
+    while done < max_steps:
+        o.step(t, w.dt)
+        t += w.dt
+        done += 1
+        if time.perf_counter() - start > budget_s:
+            break
+    elapsed = time.perf_counter() - start
+    return w.cells * done / elapsed, done, elapsed
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    max_steps = max(1, args.steps)
+    value, done, elapsed = cpu_sample(args, budget_s=args.reference_budget, max_steps=max_steps)
+    sample = f"{done} IMEX step(s) of the {args.N}x{args.N} 20-disk cavity in {elapsed:.1f} s"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": done, "warmup": 0, "ms_per_step": 1e3 * elapsed / done, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_block(args, "fp64"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_block(args, precision):
+    return {"workload": "cavity_disks20", "Nx": args.N, "Ny": args.N, "disks": 20, "phase_field": "acdi",
+            "precision": precision, "projection_reltol": args.projection_reltol,
+            "velocity_reltol": args.velocity_reltol,
+            "l2": "working set exceeds the 126 MB L2 every step; no extra flush",
+            "parallelism": f"replicas{args.gpus}"}
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    import eulerianfsi_b200 as ef
+    from eulerianfsi_b200 import _abi
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    w = build_workload(args, args.precision)
+    ctx = ef.build_imex_context(w.metrics, w.bcs, w.models, numerics=w.numerics)
+    h = ctx.handle
+    h.upload(w.state)
+    h.set_correction(np.zeros((args.N, args.N), order="F"))
+    dts = (C.c_double * max(args.warmup, args.steps, 1))(*([w.dt] * max(args.warmup, args.steps, 1)))
+    t = 0.0
+    if args.warmup:
+        h.call("step_n", t, dts, int(args.warmup), None)
+        t += args.warmup * w.dt
+    site = _abi.SITES.index(args.site)
+    h.call("set_timed_site", site)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        h.call("step_n", t, dts, int(args.steps), None)
+    torch.cuda.synchronize()
+    st = h.stats()
+    ms = st["device_ms"]
+    launches = st["kernel_launches"]
+    if dist:
+        tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * w.cells * args.steps / (ms / 1e3)
+    peak, peak_kind = _peaks()
+    site_ms = st["site_ms"] / max(st["site_launches"], 1)
+    site_bytes = st["site_bytes"] / max(st["site_launches"], 1)
+    achieved = site_bytes / (site_ms / 1e3) / 1e9 if site_ms > 0 else None
+
+    # ---- end to end through the public API with pinned host arrays ----
+    h.call("set_timed_site", -1)
+    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, args.e2e_steps))
+    pinned = []
+    for a in w.state.arrays():
+        t_ = torch.empty(a.shape[::-1], dtype=torch.float64).pin_memory()
+        arr = t_.numpy().T  # Fortran-ordered view of pinned memory
+        arr[...] = a
+        pinned.append(arr)
+    state = ef.FSIState(*pinned)
+    work = ef.allocate_imex_workspace(w.metrics)
+    qpin = torch.zeros((args.N, args.N), dtype=torch.float64).pin_memory().numpy().T
+    work.correction = qpin  # the warm start travels with the state through integrate_step
+    if e2e_steps:
+        ef.integrate_step(state, 0.0, w.dt, ctx, work)  # warm the path
+    e2e_ms = 0.0
+    for k in range(e2e_steps):
+        ef.integrate_step(state, (k + 1) * w.dt, w.dt, ctx, work)
+        e2e_ms += h.stats()["device_ms"]
+    if dist:
+        tt = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    field_bytes = sum(a.nbytes for a in state.arrays())
+    h2d = field_bytes + qpin.nbytes
+    d2h = field_bytes + qpin.nbytes
+    e2e_value = world * w.cells * e2e_steps / (e2e_ms / 1e3) if e2e_steps else None
+
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f64-state/f32-bulk", "data": "synthetic",
+        "config": config_block(args, args.precision),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_steps},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": args.site, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": args.traffic,
+                     "avg_launch_us": site_ms * 1e3, "algorithmic_bytes_per_launch": site_bytes},
+        "clocks": clocks.summary(),
+        "solver": {"projection_iterations": st["projection_iterations"],
+                   "velocity_iterations": st["velocity_iterations"]},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        v, done, el = cpu_sample(args, budget_s=args.cpu_budget, max_steps=args.cpu_steps)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                                "sample": f"{done} IMEX step(s) of the {args.N}x{args.N} workload, "
+                                          f"{el:.1f} s on one host thread"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--N", type=int, default=1024)
+    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    p.add_argument("--projection-reltol", type=float, default=1e-10)
+    p.add_argument("--velocity-reltol", type=float, default=1e-8)
+    p.add_argument("--site", default="pcg_update")
+    p.add_argument("--traffic", type=float, default=None, help="ncu dram bytes per launch of the site")
+    p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--cpu-steps", type=int, default=1)
+    p.add_argument("--cpu-budget", type=float, default=60.0)
+    p.add_argument("--reference-budget", type=float, default=150.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    args = p.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank)
+        else:
+            run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

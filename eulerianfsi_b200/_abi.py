@@ -109,7 +109,13 @@ class ProjectionResultC(Structure):
 
 class Stats(Structure):
     _fields_ = [("projection_iterations", c_int32 * 4), ("velocity_iterations", c_int32 * 4),
-                ("resource_iterations", c_int32 * 4), ("kernel_launches", c_int64)]
+                ("resource_iterations", c_int32 * 4), ("kernel_launches", c_int64),
+                ("device_ms", c_double), ("site_launches", c_int64), ("site_ms", c_double),
+                ("site_bytes", c_double)]
+
+
+SITES = ["phase", "momentum", "structure", "visc_apply", "visc_matvec", "visc_update", "pcg_matvec",
+         "pcg_update", "vcycle", "proj_rhs", "proj_finish", "combine", "vel_rhs", "finalize"]
 
 
 # Entry points shared by the CUDA library (prefix "efsi_") and the CPU oracle
@@ -133,7 +139,8 @@ SIGNATURES = {
     "get_stats": (c_int32, [_H, POINTER(Stats)]),
 }
 CUDA_ONLY = {
-    "integrate_step_host": (c_int32, [_H] + [_dp] * 7 + [c_double, c_double, POINTER(StepReportC)]),
+    "set_timed_site": (c_int32, [_H, c_int32]),
+    "integrate_step_host": (c_int32, [_H] + [_dp] * 8 + [c_double, c_double, POINTER(StepReportC)]),
     "step_n": (c_int32, [_H, c_double, _dp, c_int32, POINTER(StepReportC)]),
 }
 

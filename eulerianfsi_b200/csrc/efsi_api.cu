@@ -1,0 +1,1132 @@
+// efsi_api.cu — C-ABI of the B200 IMEX step (include/efsi.h): context creation,
+// device buffers, the four-stage orchestration of TimeIntegrationIMEX.jl:1152-1256
+// and the operator-level entry points.
+//
+// Orchestration: one CUDA stream per handle.  Every kernel of a step is enqueued
+// back to back; the Krylov solves keep their scalars on the device and are
+// enqueued in batches sized from the previous solve's iteration count, so a step
+// synchronises with the host only a few times.  Device-side errors (the Julia
+// exceptions of the reference) are raised into a status word and reported after
+// the step; a failing step leaves the state untouched.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "efsi_kernels.cuh"
+#include "efsi_solvers.cuh"
+
+using namespace efsi;
+
+namespace {
+
+struct DevBlock {
+    DevStatus st;
+    CGScal cg_visc, cg_diff, cg_proj;
+    ProjScal ps;
+    double report[6];
+    long long nonspd;
+    double max_constraint;
+    double max_trace;
+    double gamma_dyn;
+};
+
+struct Err {
+    int code;
+    std::string msg;
+};
+
+thread_local std::string g_create_error;
+
+const char* bc_name(int t) {
+    switch (t) {
+        case EFSI_BC_PERIODIC: return "Periodic";
+        case EFSI_BC_DIRICHLET: return "Dirichlet";
+        case EFSI_BC_NEUMANN: return "Neumann";
+        case EFSI_BC_MIXED: return "MixedBoundary";
+        case EFSI_BC_ADVECTIVE_OUTFLOW: return "AdvectiveOutflow";
+    }
+    return "unknown";
+}
+
+}  // namespace
+
+struct efsi_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Params P{};
+    int Nx = 0, Ny = 0;
+    size_t nc = 0, nu = 0, nv = 0;
+    std::vector<void*> allocs;
+    std::string err;
+    efsi_stats stats{};
+    bool visc = false, diff = false, growth = false, resource = false;
+    Err step_block{EFSI_OK, ""};  // why this configuration cannot step (empty: it can)
+    // state and correction
+    double *U, *V, *phi, *c, *sxx, *syy, *sxy, *q;
+    // stage buffers
+    double *Us, *Vs, *phis, *cs, *sxs, *sys, *sxys, *sxn, *syn, *sxyn, *G;
+    double *Eu[3], *Ev[3], *Iu[3], *Iv[3], *Ephi[3], *Exx[3], *Eyy[3], *Exy[3], *Ec[3], *Ic[3];
+    double *rhs_u, *rhs_v, *rhs_c;
+    double *kappa, *cap_a, *cap_b;
+    ViscSolve vs{};
+    ScalarSolve ds{};
+    Projection pj{};
+    DevBlock* dev = nullptr;   // device scalars
+    DevBlock* host = nullptr;  // pinned mirror
+    int* done_pinned = nullptr;
+    RedSlot slot[8];
+    // solver batch predictions
+    int pred_proj = 4, pred_visc = 4, pred_diff = 4;
+    long long launches = 0;
+    // CUDA-event timing: whole calls and one selectable launch site
+    cudaEvent_t call_ev[2] = {nullptr, nullptr};
+    int timed_site = EFSI_SITE_NONE;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> site_ev;
+    size_t site_used = 0;
+    double site_bytes_pending = 0.0;
+
+    template <class T>
+    T* dalloc(size_t n) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess)
+            throw Err{EFSI_CUDA, "cudaMalloc failed"};
+        cudaMemset(p, 0, std::max<size_t>(n, 1) * sizeof(T));
+        allocs.push_back(p);
+        return static_cast<T*>(p);
+    }
+    ~efsi_handle() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& e : site_ev) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+        for (cudaEvent_t e : call_ev) if (e) cudaEventDestroy(e);
+        for (void* p : allocs) cudaFree(p);
+        if (host) cudaFreeHost(host);
+        if (done_pinned) cudaFreeHost(done_pinned);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw Err{EFSI_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+void reset_call_stats(efsi_handle* h) {
+    std::memset(h->stats.projection_iterations, 0, sizeof(h->stats.projection_iterations));
+    std::memset(h->stats.velocity_iterations, 0, sizeof(h->stats.velocity_iterations));
+    std::memset(h->stats.resource_iterations, 0, sizeof(h->stats.resource_iterations));
+    h->stats.kernel_launches = 0;
+    h->stats.device_ms = 0.0;
+    h->launches = 0;
+}
+
+// Bracket a launch site with CUDA events when it is the timed one.
+template <class F>
+void site(efsi_handle* h, int which, double bytes, F&& f) {
+    if (h->timed_site != which) { f(); return; }
+    if (h->site_used == h->site_ev.size()) {
+        cudaEvent_t a, b;
+        check_cuda(cudaEventCreate(&a), "event");
+        check_cuda(cudaEventCreate(&b), "event");
+        h->site_ev.emplace_back(a, b);
+    }
+    auto& e = h->site_ev[h->site_used++];
+    check_cuda(cudaEventRecord(e.first, h->stream), "event");
+    f();
+    check_cuda(cudaEventRecord(e.second, h->stream), "event");
+    h->site_bytes_pending += bytes;
+}
+
+// After the stream is idle: fold the recorded site events into the statistics.
+void collect_site_events(efsi_handle* h) {
+    for (size_t k = 0; k < h->site_used; ++k) {
+        float ms = 0.f;
+        check_cuda(cudaEventElapsedTime(&ms, h->site_ev[k].first, h->site_ev[k].second), "event");
+        h->stats.site_ms += ms;
+        h->stats.site_launches += 1;
+    }
+    h->stats.site_bytes += h->site_bytes_pending;
+    h->site_used = 0;
+    h->site_bytes_pending = 0.0;
+}
+
+void call_begin(efsi_handle* h) { check_cuda(cudaEventRecord(h->call_ev[0], h->stream), "event"); }
+void call_end(efsi_handle* h) {
+    check_cuda(cudaEventRecord(h->call_ev[1], h->stream), "event");
+    check_cuda(cudaEventSynchronize(h->call_ev[1]), "event");
+    float ms = 0.f;
+    check_cuda(cudaEventElapsedTime(&ms, h->call_ev[0], h->call_ev[1]), "event");
+    h->stats.device_ms = ms;
+    collect_site_events(h);
+}
+
+// ---------------------------------------------------------------------------------------
+// configuration validation
+// ---------------------------------------------------------------------------------------
+double uniform_spacing(const double* a, int n, double h, const char* name) {
+    if (!a) throw Err{EFSI_ARG, std::string("mesh metric ") + name + " missing"};
+    for (int k = 0; k < n; ++k)
+        if (!(std::fabs(a[k] - h) <= 1e-12 * std::fabs(h)))
+            throw Err{EFSI_UNSUPPORTED, std::string("the device step requires uniform spacing; ") + name +
+                                            " is stretched (MeshGeneration.jl stretchings are not supported)"};
+    return h;
+}
+
+void upload_side(efsi_handle* h, const efsi_bc_side& in, int need, SideD& out, const char* what) {
+    out.type = in.type;
+    out.val = nullptr; out.neu = nullptr; out.mask = nullptr;
+    if (in.type < EFSI_BC_PERIODIC || in.type > EFSI_BC_ADVECTIVE_OUTFLOW)
+        throw Err{EFSI_ARG, std::string(what) + ": unknown boundary type"};
+    if (in.type == EFSI_BC_PERIODIC) return;
+    if (in.n < need) throw Err{EFSI_DIM, std::string(what) + ": boundary data shorter than the side"};
+    if (in.value) {
+        double* d = h->dalloc<double>(in.n);
+        check_cuda(cudaMemcpy(d, in.value, sizeof(double) * in.n, cudaMemcpyHostToDevice), "bc upload");
+        out.val = d;
+    }
+    if (in.type == EFSI_BC_MIXED) {
+        if (in.neumann) {
+            double* d = h->dalloc<double>(in.n);
+            check_cuda(cudaMemcpy(d, in.neumann, sizeof(double) * in.n, cudaMemcpyHostToDevice), "bc upload");
+            out.neu = d;
+        }
+        uint8_t* m = h->dalloc<uint8_t>(in.n);
+        if (in.mask) check_cuda(cudaMemcpy(m, in.mask, in.n, cudaMemcpyHostToDevice), "bc upload");
+        out.mask = m;
+    }
+}
+
+void upload_bcs(efsi_handle* h, const efsi_bc_setup& in, int n_lr, int n_bt, BCD& out, const char* name) {
+    const efsi_bc_side* s[4] = {&in.left, &in.right, &in.bottom, &in.top};
+    for (int k = 0; k < 4; ++k) upload_side(h, *s[k], k < 2 ? n_lr : n_bt, out.s[k], name);
+    if ((in.left.type == EFSI_BC_PERIODIC) != (in.right.type == EFSI_BC_PERIODIC))
+        throw Err{EFSI_ARG, std::string(name) + ": periodic boundaries in the x-direction must be specified as an opposing pair."};
+    if ((in.bottom.type == EFSI_BC_PERIODIC) != (in.top.type == EFSI_BC_PERIODIC))
+        throw Err{EFSI_ARG, std::string(name) + ": periodic boundaries in the y-direction must be specified as an opposing pair."};
+}
+
+bool side_has_dirichlet(const efsi_bc_side& s) {
+    if (s.type == EFSI_BC_DIRICHLET) return true;
+    if (s.type == EFSI_BC_MIXED && s.mask)
+        for (int k = 0; k < s.n; ++k)
+            if (s.mask[k]) return true;
+    return false;
+}
+
+// Requirements that only integrate_step! enforces; an empty message means the
+// configuration can step.
+Err step_requirements(const efsi_config& cfg) {
+    if (!cfg.mesh.periodic_x && cfg.bc_U.right.type != EFSI_BC_DIRICHLET)
+        return {EFSI_ARG, "The compact predictor currently requires a Dirichlet or Periodic U-right boundary."};
+    if (!cfg.mesh.periodic_y && cfg.bc_V.top.type != EFSI_BC_DIRICHLET)
+        return {EFSI_ARG, "The compact predictor currently requires a Dirichlet or Periodic V-top boundary."};
+    auto dn = [](int t) { return t == EFSI_BC_DIRICHLET || t == EFSI_BC_NEUMANN; };
+    if (!cfg.mesh.periodic_y && !(dn(cfg.bc_U.bottom.type) && dn(cfg.bc_U.top.type)))
+        return {EFSI_ARG, "Unsupported U-bottom/top boundary for du/dy: Dirichlet or Neumann required."};
+    if (!cfg.mesh.periodic_x && !(dn(cfg.bc_V.left.type) && dn(cfg.bc_V.right.type)))
+        return {EFSI_ARG, "Unsupported V-left/right boundary for dv/dx: Dirichlet or Neumann required."};
+    return {EFSI_OK, ""};
+}
+
+void validate_models(const efsi_config& cfg) {
+    const efsi_models& md = cfg.models;
+    const efsi_bc_setup* all[8] = {&cfg.bc_U, &cfg.bc_V, &cfg.bc_correction, &cfg.bc_phi, &cfg.bc_resource,
+                                   &cfg.bc_sigma_xx, &cfg.bc_sigma_yy, &cfg.bc_sigma_xy};
+    const char* names[8] = {"U", "V", "correction", "phi", "resource", "sigma_xx", "sigma_yy", "sigma_xy"};
+    for (int k = 0; k < 8; ++k) {  // TimeIntegrationIMEX.jl:447-466
+        if ((all[k]->left.type == EFSI_BC_PERIODIC) != (cfg.mesh.periodic_x != 0))
+            throw Err{EFSI_ARG, std::string(names[k]) + " boundary conditions do not match MeshMetrics periodicity in x."};
+        if ((all[k]->bottom.type == EFSI_BC_PERIODIC) != (cfg.mesh.periodic_y != 0))
+            throw Err{EFSI_ARG, std::string(names[k]) + " boundary conditions do not match MeshMetrics periodicity in y."};
+    }
+    if (md.viscosity != EFSI_VISC_NONE) {  // Operators.jl:89-105
+        const efsi_bc_side* vs[8] = {&cfg.bc_U.left, &cfg.bc_U.right, &cfg.bc_U.bottom, &cfg.bc_U.top,
+                                     &cfg.bc_V.left, &cfg.bc_V.right, &cfg.bc_V.bottom, &cfg.bc_V.top};
+        const char* vn[8] = {"U-left", "U-right", "U-bottom", "U-top", "V-left", "V-right", "V-bottom", "V-top"};
+        for (int k = 0; k < 8; ++k)
+            if (vs[k]->type != EFSI_BC_DIRICHLET && vs[k]->type != EFSI_BC_PERIODIC)
+                throw Err{EFSI_ARG, std::string(vn[k]) + " uses " + bc_name(vs[k]->type) +
+                                        ". The current compact viscous operator supports Dirichlet or Periodic velocity boundaries."};
+    }
+    // Step-only requirements (compact predictor injection, TimeIntegrationIMEX.jl:554-576;
+    // tangential velocity data of velocity_gradient / convection, Operators.jl:503-579,
+    // MomentumTransport.jl:89-102) are reported by integrate_step, as in the reference.
+    // Phase-field boundary rules (PhaseFieldMethods.jl:174-196, :493-529, :352-375).
+    const efsi_bc_side* ph[4] = {&cfg.bc_phi.left, &cfg.bc_phi.right, &cfg.bc_phi.bottom, &cfg.bc_phi.top};
+    const double tiny = 100 * 2.220446049250313e-16;
+    if (md.phase_field_method == EFSI_PF_ACDI || md.phase_field_method == EFSI_PF_UWCDI) {
+        for (const efsi_bc_side* s : ph) {
+            if (s->type == EFSI_BC_NEUMANN && s->value)
+                for (int k = 0; k < s->n; ++k)
+                    if (std::fabs(s->value[k]) > tiny)
+                        throw Err{EFSI_ARG, "Only homogeneous Neumann phase boundaries are supported by the ACDI/UWCDI operators."};
+            if (s->type == EFSI_BC_MIXED && s->neumann)
+                for (int k = 0; k < s->n; ++k)
+                    if (!(s->mask && s->mask[k]) && std::fabs(s->neumann[k]) > tiny)
+                        throw Err{EFSI_ARG, "Only homogeneous-Neumann mixed phase faces are supported here."};
+        }
+    }
+    if (md.phase_field_method == EFSI_PF_ACDI) {
+        for (const efsi_bc_side* s : ph) {
+            if (s->type == EFSI_BC_PERIODIC || s->type == EFSI_BC_NEUMANN) continue;
+            if (s->type == EFSI_BC_DIRICHLET) {
+                for (int k = 1; k < s->n; ++k)
+                    if (s->value && s->value[k] != s->value[0])
+                        throw Err{EFSI_ARG, "ACDI psi transformation currently requires scalar Dirichlet phase data."};
+                continue;
+            }
+            throw Err{EFSI_ARG, "ACDI psi geometry supports Periodic, homogeneous Neumann, or scalar Dirichlet phase boundaries."};
+        }
+    }
+    if (md.phase_field_method == EFSI_PF_UWCDI && md.pf_option == EFSI_NORMALS_SMOOTHED9) {
+        for (const efsi_bc_side* s : ph) {
+            if (s->type == EFSI_BC_PERIODIC) continue;
+            if (s->type == EFSI_BC_NEUMANN && !(s->value && std::fabs(s->value[0]) > tiny)) continue;
+            throw Err{EFSI_ARG, "smoothed9 normal reconstruction requires homogeneous Neumann or periodic phase boundaries."};
+        }
+    }
+    if (md.phase_field_method < EFSI_PF_UPWIND || md.phase_field_method > EFSI_PF_UWCDI)
+        throw Err{EFSI_ARG, "phase_field_method must be an AbstractPhaseFieldMethod."};
+}
+
+// ---------------------------------------------------------------------------------------
+// multigrid hierarchy and the dense coarse inverse
+// ---------------------------------------------------------------------------------------
+struct HostLevel {
+    int nx, ny;
+    std::vector<double> cl, cr, cb, ct;
+};
+
+double side_coef(const efsi_bc_side& s, int k) {
+    if (s.type == EFSI_BC_DIRICHLET) return 2.0;
+    if (s.type == EFSI_BC_MIXED && s.mask) return s.mask[k] ? 2.0 : 0.0;
+    return 0.0;
+}
+
+void host_level_apply(const HostLevel& L, double ax, double ay, bool px, bool py, const std::vector<double>& x,
+                      std::vector<double>& y) {
+    const int nx = L.nx, ny = L.ny;
+    y.assign((size_t)nx * ny, 0.0);
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            size_t k = (size_t)i + (size_t)j * nx;
+            double c = x[k], d = 0.0, off = 0.0;
+            if (i > 0) { d += ax; off += ax * x[k - 1]; } else if (px) { d += ax; off += ax * x[k + nx - 1]; } else d += ax * L.cl[j];
+            if (i < nx - 1) { d += ax; off += ax * x[k + 1]; } else if (px) { d += ax; off += ax * x[k - (nx - 1)]; } else d += ax * L.cr[j];
+            if (j > 0) { d += ay; off += ay * x[k - nx]; } else if (py) { d += ay; off += ay * x[k + (size_t)(ny - 1) * nx]; } else d += ay * L.cb[i];
+            if (j < ny - 1) { d += ay; off += ay * x[k + nx]; } else if (py) { d += ay; off += ay * x[k - (size_t)(ny - 1) * nx]; } else d += ay * L.ct[i];
+            y[k] = d * c - off;
+        }
+}
+
+// Inverse of the SPD (shifted if singular) coarse operator via Cholesky.
+std::vector<double> coarse_inverse(const HostLevel& L, double ax, double ay, bool px, bool py, bool singular) {
+    const int n = L.nx * L.ny;
+    std::vector<double> A((size_t)n * n, 0.0), e(n, 0.0), col;
+    for (int k = 0; k < n; ++k) {
+        e[k] = 1.0;
+        host_level_apply(L, ax, ay, px, py, e, col);
+        for (int r = 0; r < n; ++r) A[(size_t)r * n + k] = col[r];
+        e[k] = 0.0;
+    }
+    if (singular) {
+        double s = 0.0;
+        for (int k = 0; k < n; ++k) s += A[(size_t)k * n + k];
+        s /= (double)n * n;
+        for (double& a : A) a += s;
+    }
+    // lower Cholesky, row-major, in place
+    for (int j = 0; j < n; ++j) {
+        double* Aj = &A[(size_t)j * n];
+        double d = Aj[j];
+        for (int k = 0; k < j; ++k) d -= Aj[k] * Aj[k];
+        if (!(d > 0.0)) throw Err{EFSI_SOLVE, "coarse projection operator is not positive definite"};
+        d = std::sqrt(d);
+        Aj[j] = d;
+        for (int i = j + 1; i < n; ++i) {
+            double* Ai = &A[(size_t)i * n];
+            double v = Ai[j];
+            for (int k = 0; k < j; ++k) v -= Ai[k] * Aj[k];
+            Ai[j] = v / d;
+        }
+    }
+    // inverse of L (lower), then A^-1 = L^-T L^-1
+    std::vector<double> Li((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        Li[(size_t)i * n + i] = 1.0 / A[(size_t)i * n + i];
+        for (int j = 0; j < i; ++j) {
+            double s = 0.0;
+            for (int k = j; k < i; ++k) s += A[(size_t)i * n + k] * Li[(size_t)k * n + j];
+            Li[(size_t)i * n + j] = -s / A[(size_t)i * n + i];
+        }
+    }
+    std::vector<double> inv((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j <= i; ++j) {
+            double s = 0.0;
+            for (int k = i; k < n; ++k) s += Li[(size_t)k * n + i] * Li[(size_t)k * n + j];
+            inv[(size_t)i * n + j] = s;
+            inv[(size_t)j * n + i] = s;
+        }
+    return inv;
+}
+
+void build_projection(efsi_handle* h, const efsi_config& cfg) {
+    const int Nx = h->Nx, Ny = h->Ny;
+    const bool px = cfg.mesh.periodic_x, py = cfg.mesh.periodic_y;
+    const efsi_bc_setup& b = cfg.bc_correction;
+    Projection& pj = h->pj;
+    pj.nullspace = !(side_has_dirichlet(b.left) || side_has_dirichlet(b.right) || side_has_dirichlet(b.bottom) ||
+                     side_has_dirichlet(b.top));
+    std::vector<HostLevel> lv;
+    HostLevel L0;
+    L0.nx = Nx; L0.ny = Ny;
+    L0.cl.resize(Ny); L0.cr.resize(Ny); L0.cb.resize(Nx); L0.ct.resize(Nx);
+    for (int j = 0; j < Ny; ++j) { L0.cl[j] = px ? 0.0 : side_coef(b.left, j); L0.cr[j] = px ? 0.0 : side_coef(b.right, j); }
+    for (int i = 0; i < Nx; ++i) { L0.cb[i] = py ? 0.0 : side_coef(b.bottom, i); L0.ct[i] = py ? 0.0 : side_coef(b.top, i); }
+    lv.push_back(L0);
+    while (true) {
+        const HostLevel& F = lv.back();
+        if ((long)F.nx * F.ny <= 1024 || (F.nx & 1) || (F.ny & 1) || F.nx < 4 || F.ny < 4) break;
+        HostLevel C;
+        C.nx = F.nx / 2; C.ny = F.ny / 2;
+        C.cl.resize(C.ny); C.cr.resize(C.ny); C.cb.resize(C.nx); C.ct.resize(C.nx);
+        for (int j = 0; j < C.ny; ++j) { C.cl[j] = 0.5 * (F.cl[2 * j] + F.cl[2 * j + 1]); C.cr[j] = 0.5 * (F.cr[2 * j] + F.cr[2 * j + 1]); }
+        for (int i = 0; i < C.nx; ++i) { C.cb[i] = 0.5 * (F.cb[2 * i] + F.cb[2 * i + 1]); C.ct[i] = 0.5 * (F.ct[2 * i] + F.ct[2 * i + 1]); }
+        lv.push_back(C);
+        if (lv.size() >= 16) break;
+    }
+    if ((long)lv.back().nx * lv.back().ny > 1024)
+        throw Err{EFSI_UNSUPPORTED, "the projection multigrid needs grid sizes that halve down to at most 1024 coarse cells"};
+    const double ax = h->P.g.hy / h->P.g.hx, ay = h->P.g.hx / h->P.g.hy;
+    pj.nlev = (int)lv.size();
+    for (int l = 0; l < pj.nlev; ++l) {
+        MGLevel& M = pj.lev[l];
+        const HostLevel& H = lv[l];
+        M.nx = H.nx; M.ny = H.ny; M.ax = ax; M.ay = ay;
+        auto up = [&](const std::vector<double>& v) {
+            double* d = h->dalloc<double>(v.size());
+            check_cuda(cudaMemcpy(d, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice), "mg upload");
+            return d;
+        };
+        M.cl = up(H.cl); M.cr = up(H.cr); M.cb = up(H.cb); M.ct = up(H.ct);
+        size_t n = (size_t)H.nx * H.ny;
+        M.x = h->dalloc<double>(n); M.xo = h->dalloc<double>(n); M.b = h->dalloc<double>(n); M.r = h->dalloc<double>(n);
+    }
+    const HostLevel& C = lv.back();
+    std::vector<double> inv = coarse_inverse(C, ax, ay, px, py, pj.nullspace);
+    pj.nc = C.nx * C.ny;
+    pj.coarse_inv = h->dalloc<double>(inv.size());
+    check_cuda(cudaMemcpy(pj.coarse_inv, inv.data(), sizeof(double) * inv.size(), cudaMemcpyHostToDevice), "mg upload");
+    const size_t N = (size_t)Nx * Ny;
+    pj.x = h->dalloc<double>(N); pj.r = h->dalloc<double>(N); pj.z = pj.lev[0].xo;
+    pj.p[0] = h->dalloc<double>(N); pj.p[1] = h->dalloc<double>(N);
+    pj.Ap = h->dalloc<double>(N); pj.b = h->dalloc<double>(N); pj.rhs = h->dalloc<double>(N);
+    pj.Up = h->dalloc<double>(h->nu); pj.Vp = h->dalloc<double>(h->nv);
+}
+
+// ---------------------------------------------------------------------------------------
+// device status -> EFSI status
+// ---------------------------------------------------------------------------------------
+Err decode(const DevStatus& s) {
+    char buf[512];
+    static const char* fields[] = {"state.U", "state.V", "state.phi", "state.resource", "state.sigma_xx",
+                                   "state.sigma_yy", "state.sigma_xy"};
+    switch (s.code) {
+        case DE_NONFINITE_STATE:
+            snprintf(buf, sizeof buf, "%s contains non-finite values.", fields[std::min(std::max(s.where, 0), 6)]);
+            return {EFSI_ARG, buf};
+        case DE_STAGE1_CONSTRAINT:
+            snprintf(buf, sizeof buf,
+                     "The velocity entering stage 1 does not satisfy the prescribed divergence constraint. Maximum "
+                     "|div(v)-G| = %.17g. Initialize the state with make_velocity_compatible! or provide a compatible velocity.",
+                     s.value);
+            return {EFSI_ARG, buf};
+        case DE_INCOMPATIBLE:
+            snprintf(buf, sizeof buf,
+                     "The prescribed divergence constraint is incompatible with the Neumann/periodic correction "
+                     "boundaries. The volume integral of the Poisson right-hand side is %.17g.",
+                     s.value);
+            return {EFSI_ARG, buf};
+        case DE_PROJ_RESIDUAL:
+            snprintf(buf, sizeof buf,
+                     "Projection Poisson solve did not reach the required true-residual accuracy. Relative residual = %.17g, tolerance = 1e-08.",
+                     s.value);
+            return {EFSI_SOLVE, buf};
+        case DE_PROJ_CONSTRAINT:
+            snprintf(buf, sizeof buf, "Projection did not satisfy the prescribed divergence constraint. Weighted L2 residual = %.17g.", s.value);
+            return {EFSI_SOLVE, buf};
+        case DE_NON_SPD:
+            snprintf(buf, sizeof buf,
+                     "GeometricStructureExtension requires an SPD tensor; encountered a non-positive or non-finite eigenvalue (cell %d,%d).",
+                     s.i + 1, s.j + 1);
+            return {EFSI_DOMAIN, buf};
+        case DE_NEUMANN_INFLOW:
+            snprintf(buf, sizeof buf,
+                     "A Neumann condition does not define the incoming advected state at face (%d,%d). Prescribe Dirichlet data for advective inflow.",
+                     s.i + 1, s.j + 1);
+            return {EFSI_ARG, buf};
+        case DE_BAD_VISCOSITY: return {EFSI_ARG, "evaluated viscosity must be strictly positive everywhere."};
+        case DE_BAD_DIFFUSIVITY: return {EFSI_ARG, "evaluated diffusivity must be strictly positive everywhere."};
+        case DE_NONFINITE_SINK: return {EFSI_ARG, "Evaluated resource sink contains non-finite values."};
+        case DE_LINEAR_NOCONV:
+            snprintf(buf, sizeof buf, "%s linear solve did not converge (residual %.3g).",
+                     s.where == 0 ? "velocity" : (s.where == 1 ? "resource" : "projection"), s.value);
+            return {EFSI_SOLVE, buf};
+        default:
+            snprintf(buf, sizeof buf, "device error %d", s.code);
+            return {EFSI_ARG, buf};
+    }
+}
+
+void fetch_dev(efsi_handle* h) {
+    check_cuda(cudaMemcpyAsync(h->host, h->dev, sizeof(DevBlock), cudaMemcpyDeviceToHost, h->stream), "readback");
+    check_cuda(cudaStreamSynchronize(h->stream), "step");
+}
+
+void raise_if_failed(efsi_handle* h) {
+    if (h->host->st.code != 0) {
+        Err e = decode(h->host->st);
+        throw e;
+    }
+}
+
+// Zero the per-call scalars (status, maxima).
+__global__ void k_reset_block(DevBlock* d) {
+    d->st.code = 0;
+    d->max_constraint = 0.0;
+    d->max_trace = 0.0;
+}
+
+// ---------------------------------------------------------------------------------------
+// CG drivers: enqueue predicted iterations, then confirm `done` on the host
+// ---------------------------------------------------------------------------------------
+template <class Iter>
+int run_cg(efsi_handle* h, CGScal* cg, int maxiter, int& pred, Iter&& iter, int kernels_per_iter, int where) {
+    int it = 0;
+    int batch = std::max(1, std::min(pred, maxiter));
+    int* flags = h->done_pinned;  // iter, done, maxiter, conv (CGScal order)
+    while (true) {
+        int k = 0;
+        for (; k < batch && it < maxiter; ++k, ++it) iter(it);
+        h->launches += (long long)k * kernels_per_iter;
+        check_cuda(cudaMemcpyAsync(flags, &cg->iter, 4 * sizeof(int), cudaMemcpyDeviceToHost, h->stream),
+                   "cg readback");
+        check_cuda(cudaStreamSynchronize(h->stream), "cg");
+        if (flags[1] || it >= maxiter) break;
+        batch = 2;
+    }
+    const int iters = flags[0], conv = flags[3];
+    pred = std::max(1, iters);
+    (void)where;
+    return conv ? iters : -iters;
+}
+
+StageFields stage_fields(const double* U, const double* V, const double* phi, const double* c, const double* sxx,
+                         const double* syy, const double* sxy, const double* G) {
+    return StageFields{U, V, phi, c, sxx, syy, sxy, G};
+}
+
+// Algorithmic bytes (unique FP64 reads + writes once) of one V-cycle.
+double vcycle_bytes(const Projection& pj) {
+    double b = 0.0;
+    for (int l = 0; l + 1 < pj.nlev; ++l) {
+        double n = (double)pj.lev[l].nx * pj.lev[l].ny, nc = (double)pj.lev[l + 1].nx * pj.lev[l + 1].ny;
+        b += 10.5 * n + 2.0 * nc;
+    }
+    double nc = pj.nc;
+    return 8.0 * (b + nc * nc + 2.0 * nc);
+}
+
+// One projection of (compact predictor | full arrays) onto div = G, writing U_out/V_out/q.
+void projection(efsi_handle* h, bool compact, const double* u_in, const double* v_in, const double* G, double* U_out,
+                double* V_out, int stage_slot) {
+    const Params& P = h->P;
+    DevBlock* d = h->dev;
+    const double N = (double)h->nc, nuv = (double)(h->nu + h->nv), g = G ? 1.0 : 0.0;
+    site(h, EFSI_SITE_PROJ_RHS, 8.0 * (2.0 * nuv + N * (2.0 + g)),
+         [&] { proj_rhs(P, h->pj, compact, u_in, v_in, G, &d->ps, h->slot[0], &d->st, h->stream); });
+    proj_cg_init(P, h->pj, P.nu.projection_reltol, P.nu.projection_maxiter, h->q, &d->cg_proj, &d->ps, h->slot[1],
+                 h->slot[2], &d->st, h->stream);
+    h->launches += 2 + 6 * (h->pj.nlev - 1) + 1;
+    const double vb = vcycle_bytes(h->pj);
+    int iters = run_cg(
+        h, &d->cg_proj, P.nu.projection_maxiter, h->pred_proj,
+        [&](int it) {
+            site(h, EFSI_SITE_PCG_MATVEC, 8.0 * N * (it == 0 ? 3.0 : 4.0),
+                 [&] { proj_matvec(P, h->pj, it, &d->cg_proj, h->slot[3], h->stream); });
+            site(h, EFSI_SITE_PCG_UPDATE, 8.0 * N * 6.0,
+                 [&] { proj_update(P, h->pj, it, &d->cg_proj, h->slot[4], h->stream); });
+            site(h, EFSI_SITE_VCYCLE, vb, [&] { proj_vcycle(P, h->pj, &d->cg_proj, h->slot[5], h->stream); });
+        },
+        proj_kernels_per_iter(h->pj), 2);
+    h->stats.projection_iterations[stage_slot] = std::abs(iters);
+    site(h, EFSI_SITE_PROJ_FINISH, 8.0 * (4.0 * N + 2.0 * nuv + g * N), [&] {
+        proj_finish(P, h->pj, G, h->q, U_out, V_out, &d->ps, &d->max_constraint, h->slot[6], h->slot[7], &d->st,
+                    h->stream);
+    });
+    h->launches += 3;
+}
+
+void tendencies(efsi_handle* h, int s, double t_stage, const StageFields& f) {
+    const Params& P = h->P;
+    DevBlock* d = h->dev;
+    const double N = (double)h->nc, nuv = (double)(h->nu + h->nv), g = f.G ? 1.0 : 0.0;
+    const double* kappa = nullptr;
+    if (P.md.capillarity == EFSI_CAP_DIFFUSE_AREA) {
+        launch_capillary_curvature(P, f.phi, h->cap_a, h->cap_b, h->kappa, h->stream);
+        kappa = h->kappa;
+        h->launches += 1 + P.md.capillary_smoothing_passes;
+    }
+    site(h, EFSI_SITE_MOMENTUM, 8.0 * (nuv + N * (4.0 + g) + 2.0 * N),
+         [&] { launch_momentum_rhs(P, t_stage, f, kappa, h->Eu[s], h->Ev[s], &d->st, h->stream); });
+    if (P.md.phase_field_method == EFSI_PF_ACDI && P.md.pf_option) {
+        launch_umax(P, f.U, f.V, &d->gamma_dyn, h->slot[0], h->stream);
+        h->launches += 1;
+    }
+    site(h, EFSI_SITE_PHASE, 8.0 * (nuv + N * (2.0 + g)),
+         [&] { launch_phase_rhs(P, f, &d->gamma_dyn, h->Ephi[s], &d->st, h->stream); });
+    if (h->resource) launch_resource_rhs(P, f, h->Ec[s], h->diff ? h->Ic[s] : nullptr, &d->st, h->stream);
+    site(h, EFSI_SITE_STRUCTURE, 8.0 * (nuv + N * (4.0 + g) + 3.0 * N),
+         [&] { launch_structure_rhs(P, f, h->Exx[s], h->Eyy[s], h->Exy[s], &d->st, h->stream); });
+    if (h->visc)
+        site(h, EFSI_SITE_VISC_APPLY, 8.0 * N * (4.0 + (P.md.viscosity == EFSI_VISC_HARMONIC ? 1.0 : 0.0)),
+             [&] { launch_viscous_apply(P, f.U, f.V, f.phi, h->Iu[s], h->Iv[s], h->stream); });
+    h->launches += 3 + (h->resource ? 1 : 0) + (h->visc ? 1 : 0);
+}
+
+const double c_AI_diag[4] = {0.0, 4.0 / 15, 1.0 / 15, 1.0 / 6};
+const double c_CS[4] = {0.0, 8.0 / 15, 2.0 / 3, 1.0};
+
+void enqueue_step(efsi_handle* h, double t, double dt) {
+    const Params& P = h->P;
+    DevBlock* d = h->dev;
+    cudaStream_t s = h->stream;
+    std::memset(h->stats.projection_iterations, 0, sizeof(h->stats.projection_iterations));
+    std::memset(h->stats.velocity_iterations, 0, sizeof(h->stats.velocity_iterations));
+    std::memset(h->stats.resource_iterations, 0, sizeof(h->stats.resource_iterations));
+    k_reset_block<<<1, 1, 0, s>>>(d);
+    launch_prepare_step(P, h->U, h->V, h->phi, h->c, h->sxx, h->syy, h->sxy, h->sxn, h->syn, h->sxyn, &d->st, s);
+    h->launches += 2;
+    const double* Gp = h->growth ? h->G : nullptr;
+    for (int st = 0; st < 4; ++st) {
+        StageFields f;
+        if (st == 0) {
+            f = stage_fields(h->U, h->V, h->phi, h->c, h->sxn, h->syn, h->sxyn, Gp);
+        } else {
+            bool rc = h->resource;
+            const double nE = (st == 1) ? 1.0 : 2.0;
+            site(h, EFSI_SITE_COMBINE, 8.0 * (double)h->nc * (4.0 + 4.0 * nE + 4.0 + (rc ? 2.0 + 2.0 * st : 0.0)), [&] {
+                launch_combine_scalars(P, st, dt, h->phi, h->sxn, h->syn, h->sxyn, h->c, h->Ephi, h->Exx, h->Eyy,
+                                       h->Exy, rc ? h->Ec : nullptr, (rc && h->diff) ? h->Ic : nullptr, h->phis,
+                                       h->sxs, h->sys, h->sxys, rc ? (h->diff ? h->rhs_c : h->cs) : nullptr, s);
+            });
+            h->launches += 1;
+            const double* cstage = h->c;
+            if (rc) {
+                cstage = h->cs;
+                if (h->diff) {
+                    double alpha = dt * c_AI_diag[st];
+                    diff_init(P, alpha, P.nu.linear_reltol, std::max(1, P.nu.linear_maxiter), h->c, h->rhs_c, h->phis,
+                              h->ds, &d->cg_diff, h->slot[0], s);
+                    h->launches += 1;
+                    int it = run_cg(
+                        h, &d->cg_diff, std::max(1, P.nu.linear_maxiter), h->pred_diff,
+                        [&](int k) { diff_iter(P, alpha, h->phis, h->ds, k, &d->cg_diff, h->slot[1], h->slot[2], s); },
+                        3, 1);
+                    h->stats.resource_iterations[st] = std::abs(it);
+                }
+            }
+            f = stage_fields(h->Us, h->Vs, h->phis, cstage, h->sxs, h->sys, h->sxys, Gp);
+        }
+        if (h->growth) {
+            launch_growth(P, f.phi, f.c, h->G, &d->max_trace, h->slot[0], s);
+            h->launches += 1;
+        }
+        if (st == 0) {
+            launch_stage1_check(P, h->U, h->V, Gp, &d->max_constraint, h->slot[0], &d->st, s);
+            h->launches += 1;
+        } else {
+            site(h, EFSI_SITE_VEL_RHS, 8.0 * (double)h->nc * (4.0 + 4.0 * st), [&] {
+                launch_velocity_rhs(P, st, dt, h->U, h->V, h->Eu, h->Ev, h->Iu, h->Iv, h->phis, h->rhs_u, h->rhs_v,
+                                    s);
+            });
+            h->launches += 1;
+            if (h->visc) {
+                double alpha = dt * c_AI_diag[st];
+                visc_init(P, alpha, P.nu.linear_reltol, std::max(1, P.nu.linear_maxiter), h->U, h->V, h->rhs_u,
+                          h->rhs_v, h->phis, h->vs, &d->cg_visc, h->slot[0], s);
+                h->launches += 2;
+                int it = run_cg(
+                    h, &d->cg_visc, std::max(1, P.nu.linear_maxiter), h->pred_visc,
+                    [&](int k) {
+                        const double N = (double)h->nc;
+                        site(h, EFSI_SITE_VISC_MATVEC, 8.0 * N * (k == 0 ? 10.0 : 12.0), [&] {
+                            visc_matvec(P, alpha, h->phis, h->vs, k, &d->cg_visc, h->slot[1], s);
+                        });
+                        site(h, EFSI_SITE_VISC_UPDATE, 8.0 * N * 14.0, [&] {
+                            visc_update(P, alpha, h->phis, h->vs, k, &d->cg_visc, h->slot[2], s);
+                        });
+                    },
+                    3, 0);
+                h->stats.velocity_iterations[st] = std::abs(it);
+            } else {
+                visc_enforce_dirichlet(P, h->rhs_u, h->rhs_v, h->vs.x_u, h->vs.x_v, s);
+                h->launches += 1;
+            }
+            projection(h, true, h->vs.x_u, h->vs.x_v, Gp, h->Us, h->Vs, st);
+        }
+        if (st < 3) tendencies(h, st, t + c_CS[st] * dt, f);
+    }
+    site(h, EFSI_SITE_FINALIZE, 16.0 * (double)(h->nu + h->nv + 5 * h->nc), [&] {
+        launch_finalize(P, h->Us, h->Vs, h->phis, h->resource ? h->cs : h->c, h->sxs, h->sys, h->sxys, h->U, h->V,
+                        h->phi, h->c, h->sxx, h->syy, h->sxy, d->report, &d->nonspd, h->slot[0], h->slot[1], &d->st,
+                        s);
+    });
+    h->launches += 1;
+    h->stats.kernel_launches = h->launches;
+}
+
+void fill_report(efsi_handle* h, efsi_step_report* r) {
+    if (!r) return;
+    const DevBlock& b = *h->host;
+    r->maximum_projection_constraint_linf = b.max_constraint;
+    r->maximum_growth_trace_error = b.max_trace;
+    r->minimum_phi = b.report[0];
+    r->maximum_phi = b.report[1];
+    r->minimum_resource = b.report[2];
+    r->minimum_sigma_eigenvalue = b.report[3];
+    r->maximum_abs_sigma_determinant_error = b.report[4];
+    r->non_spd_cells = b.nonspd;
+}
+
+template <class F>
+int guarded(efsi_handle* h, F&& f) {
+    try {
+        if (h) check_cuda(cudaSetDevice(h->device), "cudaSetDevice");
+        f();
+        return EFSI_OK;
+    } catch (const Err& e) {
+        if (h) h->err = e.msg; else g_create_error = e.msg;
+        return e.code;
+    } catch (const std::exception& e) {
+        if (h) h->err = e.what(); else g_create_error = e.what();
+        return EFSI_CUDA;
+    }
+}
+
+void h2d(efsi_handle* h, double* dst, const double* src, size_t n) {
+    check_cuda(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, h->stream), "upload");
+}
+void d2h(efsi_handle* h, double* dst, const double* src, size_t n) {
+    check_cuda(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "download");
+}
+
+}  // namespace
+
+// =========================================================================================
+// C entry points
+// =========================================================================================
+extern "C" {
+
+int efsi_create(const efsi_config* cfg, efsi_handle** out) {
+    if (out) *out = nullptr;
+    auto h = std::make_unique<efsi_handle>();
+    int st = guarded(nullptr, [&] {
+        if (!cfg || !out) throw Err{EFSI_ARG, "config and output handle must not be NULL"};
+        if (cfg->abi_version != EFSI_ABI_VERSION) throw Err{EFSI_ARG, "efsi_config ABI version mismatch"};
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw Err{EFSI_CUDA, "no CUDA device is available"};
+        check_cuda(cudaGetDevice(&h->device), "cudaGetDevice");
+        const efsi_mesh& m = cfg->mesh;
+        if (m.Nx < 2) throw Err{EFSI_ARG, "Nx must be at least 2."};
+        if (m.Ny < 2) throw Err{EFSI_ARG, "Ny must be at least 2."};
+        h->Nx = m.Nx; h->Ny = m.Ny;
+        const double hx = m.Lx / m.Nx, hy = m.Ly / m.Ny;
+        uniform_spacing(m.dx_c, m.Nx, hx, "dx_c");
+        uniform_spacing(m.dy_c, m.Ny, hy, "dy_c");
+        uniform_spacing(m.dx_f, m.Nx + 1, hx, "dx_f");
+        uniform_spacing(m.dy_f, m.Ny + 1, hy, "dy_f");
+        validate_models(*cfg);
+        h->step_block = step_requirements(*cfg);
+        check_cuda(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
+        check_cuda(cudaEventCreate(&h->call_ev[0]), "event");
+        check_cuda(cudaEventCreate(&h->call_ev[1]), "event");
+        Params& P = h->P;
+        P.g = GridD{m.Nx, m.Ny, m.periodic_x ? 1 : 0, m.periodic_y ? 1 : 0, hx, hy, 1.0 / hx, 1.0 / hy, m.Lx, m.Ly};
+        const int Nx = m.Nx, Ny = m.Ny;
+        upload_bcs(h.get(), cfg->bc_U, Ny, Nx + 1, P.bu, "U");
+        upload_bcs(h.get(), cfg->bc_V, Ny + 1, Nx, P.bv, "V");
+        upload_bcs(h.get(), cfg->bc_correction, Ny, Nx, P.bq, "correction");
+        upload_bcs(h.get(), cfg->bc_phi, Ny, Nx, P.bphi, "phi");
+        upload_bcs(h.get(), cfg->bc_resource, Ny, Nx, P.bc, "resource");
+        upload_bcs(h.get(), cfg->bc_sigma_xx, Ny, Nx, P.bsxx, "sigma_xx");
+        upload_bcs(h.get(), cfg->bc_sigma_yy, Ny, Nx, P.bsyy, "sigma_yy");
+        upload_bcs(h.get(), cfg->bc_sigma_xy, Ny, Nx, P.bsxy, "sigma_xy");
+        P.md = cfg->models;
+        P.nu = cfg->numerics;
+        if (P.md.growth_tensor == EFSI_GTENSOR_DIRECTIONAL) {  // normalised as in GrowthModels.jl:154-167
+            double tx = P.md.growth_direction_x, ty = P.md.growth_direction_y, mag = std::hypot(tx, ty);
+            if (!(mag > 0.0)) throw Err{EFSI_ARG, "Directional growth requires a non-zero direction vector."};
+            P.md.growth_direction_x = tx / mag;
+            P.md.growth_direction_y = ty / mag;
+        }
+        if (P.md.phase_field_method == EFSI_PF_ACDI) {
+            const efsi_bc_side* ph[4] = {&cfg->bc_phi.left, &cfg->bc_phi.right, &cfg->bc_phi.bottom, &cfg->bc_phi.top};
+            for (int k = 0; k < 4; ++k) {
+                P.psi_bc[k] = 0.0;
+                if (ph[k]->type == EFSI_BC_DIRICHLET && ph[k]->value) {
+                    double p = std::min(std::max(ph[k]->value[0], 0.0), 1.0), e = P.md.pf_param[2];
+                    P.psi_bc[k] = P.md.pf_param[1] * std::log((p + e) / (1.0 - p + e));
+                }
+            }
+        }
+        if (!(P.nu.projection_reltol > 0)) throw Err{EFSI_ARG, "projection_reltol must be positive."};
+        if (!(P.nu.projection_maxiter > 0)) throw Err{EFSI_ARG, "projection_maxiter must be positive."};
+        if (!(P.nu.linear_reltol > 0)) throw Err{EFSI_ARG, "Linear-solver reltol must be positive."};
+        h->visc = P.md.viscosity != EFSI_VISC_NONE;
+        h->diff = P.md.diffusivity != EFSI_DIFF_NONE;
+        h->growth = P.md.growth_source != EFSI_GROWTH_NONE;
+        h->resource = !(P.md.growth_source == EFSI_GROWTH_NONE && P.md.diffusivity == EFSI_DIFF_NONE &&
+                        P.md.resource_consumption == EFSI_CONSUMPTION_NONE);
+        const size_t N = (size_t)Nx * Ny;
+        h->nc = N; h->nu = (size_t)(Nx + 1) * Ny; h->nv = (size_t)Nx * (Ny + 1);
+        h->U = h->dalloc<double>(h->nu); h->V = h->dalloc<double>(h->nv);
+        h->phi = h->dalloc<double>(N); h->c = h->dalloc<double>(N);
+        h->sxx = h->dalloc<double>(N); h->syy = h->dalloc<double>(N); h->sxy = h->dalloc<double>(N);
+        h->q = h->dalloc<double>(N);
+        h->Us = h->dalloc<double>(h->nu); h->Vs = h->dalloc<double>(h->nv);
+        h->phis = h->dalloc<double>(N); h->cs = h->dalloc<double>(N);
+        h->sxs = h->dalloc<double>(N); h->sys = h->dalloc<double>(N); h->sxys = h->dalloc<double>(N);
+        h->sxn = h->dalloc<double>(N); h->syn = h->dalloc<double>(N); h->sxyn = h->dalloc<double>(N);
+        h->G = h->dalloc<double>(N);
+        for (int k = 0; k < 3; ++k) {
+            h->Eu[k] = h->dalloc<double>(N); h->Ev[k] = h->dalloc<double>(N);
+            h->Iu[k] = h->dalloc<double>(N); h->Iv[k] = h->dalloc<double>(N);
+            h->Ephi[k] = h->dalloc<double>(N);
+            h->Exx[k] = h->dalloc<double>(N); h->Eyy[k] = h->dalloc<double>(N); h->Exy[k] = h->dalloc<double>(N);
+            h->Ec[k] = h->resource ? h->dalloc<double>(N) : nullptr;
+            h->Ic[k] = (h->resource && h->diff) ? h->dalloc<double>(N) : nullptr;
+        }
+        h->rhs_u = h->dalloc<double>(N); h->rhs_v = h->dalloc<double>(N); h->rhs_c = h->dalloc<double>(N);
+        if (P.md.capillarity == EFSI_CAP_DIFFUSE_AREA) {
+            h->kappa = h->dalloc<double>(N); h->cap_a = h->dalloc<double>(N); h->cap_b = h->dalloc<double>(N);
+        }
+        ViscSolve& vs = h->vs;
+        vs.x_u = h->dalloc<double>(N); vs.x_v = h->dalloc<double>(N);
+        vs.r_u = h->dalloc<double>(N); vs.r_v = h->dalloc<double>(N);
+        for (int k = 0; k < 2; ++k) { vs.p_u[k] = h->dalloc<double>(N); vs.p_v[k] = h->dalloc<double>(N); }
+        vs.Ap_u = h->dalloc<double>(N); vs.Ap_v = h->dalloc<double>(N);
+        vs.dinv_u = h->dalloc<double>(N); vs.dinv_v = h->dalloc<double>(N);
+        ScalarSolve& ds = h->ds;
+        ds.x = h->cs; ds.r = h->dalloc<double>(N);
+        ds.p[0] = h->dalloc<double>(N); ds.p[1] = h->dalloc<double>(N); ds.Ap = h->dalloc<double>(N);
+        ds.dinv = h->dalloc<double>(N);
+        build_projection(h.get(), *cfg);
+        // reduction slots sized for the largest launch grid ((Nx+1) x (Ny+1) points, 32x8 blocks)
+        int maxBlocks = ((Nx + 1 + 31) / 32) * ((Ny + 1 + 7) / 8);
+        for (RedSlot& r : h->slot) {
+            r.part = h->dalloc<double>((size_t)maxBlocks * 6);
+            r.ticket = h->dalloc<unsigned>(1);
+            r.maxBlocks = maxBlocks;
+        }
+        h->dev = h->dalloc<DevBlock>(1);
+        check_cuda(cudaMallocHost(&h->host, sizeof(DevBlock)), "pinned");
+        check_cuda(cudaMallocHost(&h->done_pinned, 4 * sizeof(int)), "pinned");
+        std::memset(h->host, 0, sizeof(DevBlock));
+        // default state: rest, sigma = I (the workspace's initial values)
+        std::vector<double> ones(N, 1.0);
+        check_cuda(cudaMemcpy(h->sxx, ones.data(), N * sizeof(double), cudaMemcpyHostToDevice), "init");
+        check_cuda(cudaMemcpy(h->syy, ones.data(), N * sizeof(double), cudaMemcpyHostToDevice), "init");
+        check_cuda(cudaDeviceSynchronize(), "create");
+        *out = h.release();
+    });
+    return st;
+}
+
+void efsi_destroy(efsi_handle* h) { delete h; }
+
+const char* efsi_last_error(const efsi_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int efsi_upload_state(efsi_handle* h, const double* U, const double* V, const double* phi, const double* c,
+                      const double* sxx, const double* syy, const double* sxy) {
+    return guarded(h, [&] {
+        if (!U || !V || !phi || !sxx || !syy || !sxy) throw Err{EFSI_ARG, "state arrays must not be NULL"};
+        h2d(h, h->U, U, h->nu); h2d(h, h->V, V, h->nv); h2d(h, h->phi, phi, h->nc);
+        if (c) h2d(h, h->c, c, h->nc);
+        else check_cuda(cudaMemsetAsync(h->c, 0, h->nc * sizeof(double), h->stream), "upload");
+        h2d(h, h->sxx, sxx, h->nc); h2d(h, h->syy, syy, h->nc); h2d(h, h->sxy, sxy, h->nc);
+        check_cuda(cudaStreamSynchronize(h->stream), "upload");
+    });
+}
+
+int efsi_download_state(efsi_handle* h, double* U, double* V, double* phi, double* c, double* sxx, double* syy,
+                        double* sxy) {
+    return guarded(h, [&] {
+        if (U) d2h(h, U, h->U, h->nu);
+        if (V) d2h(h, V, h->V, h->nv);
+        if (phi) d2h(h, phi, h->phi, h->nc);
+        if (c) d2h(h, c, h->c, h->nc);
+        if (sxx) d2h(h, sxx, h->sxx, h->nc);
+        if (syy) d2h(h, syy, h->syy, h->nc);
+        if (sxy) d2h(h, sxy, h->sxy, h->nc);
+        check_cuda(cudaStreamSynchronize(h->stream), "download");
+    });
+}
+
+int efsi_set_correction(efsi_handle* h, const double* q) {
+    return guarded(h, [&] {
+        if (q) h2d(h, h->q, q, h->nc);
+        else check_cuda(cudaMemsetAsync(h->q, 0, h->nc * sizeof(double), h->stream), "correction");
+        check_cuda(cudaStreamSynchronize(h->stream), "correction");
+    });
+}
+
+int efsi_get_correction(efsi_handle* h, double* q) {
+    return guarded(h, [&] {
+        d2h(h, q, h->q, h->nc);
+        check_cuda(cudaStreamSynchronize(h->stream), "correction");
+    });
+}
+
+int efsi_make_velocity_compatible(efsi_handle* h, efsi_projection_result* r) {
+    return guarded(h, [&] {
+        const Params& P = h->P;
+        DevBlock* d = h->dev;
+        reset_call_stats(h);
+        call_begin(h);
+        k_reset_block<<<1, 1, 0, h->stream>>>(d);
+        launch_prepare_step(P, h->U, h->V, h->phi, h->c, h->sxx, h->syy, h->sxy, h->sxn, h->syn, h->sxyn, &d->st,
+                            h->stream);
+        const double* Gp = nullptr;
+        if (h->growth) {
+            launch_growth(P, h->phi, h->c, h->G, &d->max_trace, h->slot[0], h->stream);
+            Gp = h->G;
+        }
+        // project! of state.U/V in place: the predictor is copied to Up/Vp first.
+        projection(h, false, h->U, h->V, Gp, h->U, h->V, 0);
+        call_end(h);
+        fetch_dev(h);
+        raise_if_failed(h);
+        if (r) {
+            r->linear_relative_residual = h->host->ps.v[7];
+            r->constraint_linf = h->host->ps.v[8];
+            r->constraint_l2 = h->host->ps.v[9];
+            r->compatibility_defect = h->pj.nullspace ? h->host->ps.v[0] : 0.0;
+        }
+        h->stats.kernel_launches = h->launches;
+    });
+}
+
+int efsi_integrate_step(efsi_handle* h, double t, double dt, efsi_step_report* report) {
+    return guarded(h, [&] {
+        if (!std::isfinite(t)) throw Err{EFSI_ARG, "t must be finite."};
+        if (!std::isfinite(dt)) throw Err{EFSI_ARG, "dt must be finite."};
+        if (!(dt > 0)) throw Err{EFSI_ARG, "dt must be strictly positive."};
+        if (h->step_block.code != EFSI_OK) throw h->step_block;
+        reset_call_stats(h);
+        call_begin(h);
+        enqueue_step(h, t, dt);
+        call_end(h);
+        fetch_dev(h);
+        raise_if_failed(h);
+        fill_report(h, report);
+    });
+}
+
+int efsi_integrate_step_host(efsi_handle* h, double* U, double* V, double* phi, double* c, double* sxx, double* syy,
+                             double* sxy, double* q, double t, double dt, efsi_step_report* report) {
+    return guarded(h, [&] {
+        if (!U || !V || !phi || !sxx || !syy || !sxy) throw Err{EFSI_ARG, "state arrays must not be NULL"};
+        if (!std::isfinite(t)) throw Err{EFSI_ARG, "t must be finite."};
+        if (!std::isfinite(dt)) throw Err{EFSI_ARG, "dt must be finite."};
+        if (!(dt > 0)) throw Err{EFSI_ARG, "dt must be strictly positive."};
+        if (h->step_block.code != EFSI_OK) throw h->step_block;
+        reset_call_stats(h);
+        call_begin(h);
+        h2d(h, h->U, U, h->nu); h2d(h, h->V, V, h->nv); h2d(h, h->phi, phi, h->nc);
+        if (c) h2d(h, h->c, c, h->nc);
+        else check_cuda(cudaMemsetAsync(h->c, 0, h->nc * sizeof(double), h->stream), "upload");
+        h2d(h, h->sxx, sxx, h->nc); h2d(h, h->syy, syy, h->nc); h2d(h, h->sxy, sxy, h->nc);
+        if (q) h2d(h, h->q, q, h->nc);
+        enqueue_step(h, t, dt);
+        fetch_dev(h);
+        if (h->host->st.code != 0) {
+            call_end(h);
+            throw decode(h->host->st);
+        }
+        d2h(h, U, h->U, h->nu); d2h(h, V, h->V, h->nv); d2h(h, phi, h->phi, h->nc);
+        if (c) d2h(h, c, h->c, h->nc);
+        d2h(h, sxx, h->sxx, h->nc); d2h(h, syy, h->syy, h->nc); d2h(h, sxy, h->sxy, h->nc);
+        if (q) d2h(h, q, h->q, h->nc);
+        call_end(h);
+        fill_report(h, report);
+    });
+}
+
+int efsi_step_n(efsi_handle* h, double t0, const double* dts, int32_t n, efsi_step_report* reports) {
+    return guarded(h, [&] {
+        if (n < 0 || (n > 0 && !dts)) throw Err{EFSI_ARG, "dts must hold n step sizes"};
+        if (h->step_block.code != EFSI_OK) throw h->step_block;
+        for (int k = 0; k < n; ++k)
+            if (!std::isfinite(dts[k]) || !(dts[k] > 0)) throw Err{EFSI_ARG, "dt must be finite and strictly positive."};
+        double t = t0;
+        long long launches = 0;
+        int32_t it_proj[4] = {0, 0, 0, 0}, it_visc[4] = {0, 0, 0, 0};
+        reset_call_stats(h);
+        call_begin(h);  // one event pair spans all n steps, host round trips included
+        for (int k = 0; k < n; ++k) {
+            h->launches = 0;
+            enqueue_step(h, t, dts[k]);
+            launches += h->launches;
+            for (int q = 0; q < 4; ++q) {
+                it_proj[q] += h->stats.projection_iterations[q];
+                it_visc[q] += h->stats.velocity_iterations[q];
+            }
+            fetch_dev(h);
+            if (h->host->st.code != 0) {
+                call_end(h);
+                Err e = decode(h->host->st);
+                e.msg = "step " + std::to_string(k + 1) + " of " + std::to_string(n) + ": " + e.msg;
+                throw e;
+            }
+            if (reports) fill_report(h, &reports[k]);
+            t += dts[k];
+        }
+        call_end(h);
+        h->stats.kernel_launches = launches;
+        for (int q = 0; q < 4; ++q) {  // summed over the n steps
+            h->stats.projection_iterations[q] = it_proj[q];
+            h->stats.velocity_iterations[q] = it_visc[q];
+        }
+    });
+}
+
+int efsi_project(efsi_handle* h, double* U, double* V, const double* target, efsi_projection_result* r) {
+    return guarded(h, [&] {
+        DevBlock* d = h->dev;
+        k_reset_block<<<1, 1, 0, h->stream>>>(d);
+        h2d(h, h->Us, U, h->nu);
+        h2d(h, h->Vs, V, h->nv);
+        const double* Gp = nullptr;
+        if (target) { h2d(h, h->G, target, h->nc); Gp = h->G; }
+        projection(h, false, h->Us, h->Vs, Gp, h->Us, h->Vs, 0);
+        fetch_dev(h);
+        raise_if_failed(h);
+        d2h(h, U, h->Us, h->nu);
+        d2h(h, V, h->Vs, h->nv);
+        check_cuda(cudaStreamSynchronize(h->stream), "project");
+        if (r) {
+            r->linear_relative_residual = h->host->ps.v[7];
+            r->constraint_linf = h->host->ps.v[8];
+            r->constraint_l2 = h->host->ps.v[9];
+            r->compatibility_defect = h->pj.nullspace ? h->host->ps.v[0] : 0.0;
+        }
+    });
+}
+
+int efsi_phase_field_rhs(efsi_handle* h, const double* U, const double* V, const double* phi, const double* G,
+                         double* rhs) {
+    return guarded(h, [&] {
+        DevBlock* d = h->dev;
+        k_reset_block<<<1, 1, 0, h->stream>>>(d);
+        h2d(h, h->Us, U, h->nu); h2d(h, h->Vs, V, h->nv); h2d(h, h->phis, phi, h->nc);
+        const double* Gp = nullptr;
+        if (G) { h2d(h, h->G, G, h->nc); Gp = h->G; }
+        StageFields f = stage_fields(h->Us, h->Vs, h->phis, h->c, h->sxs, h->sys, h->sxys, Gp);
+        if (h->P.md.phase_field_method == EFSI_PF_ACDI && h->P.md.pf_option)
+            launch_umax(h->P, f.U, f.V, &d->gamma_dyn, h->slot[0], h->stream);
+        launch_phase_rhs(h->P, f, &d->gamma_dyn, h->Ephi[0], &d->st, h->stream);
+        fetch_dev(h);
+        raise_if_failed(h);
+        d2h(h, rhs, h->Ephi[0], h->nc);
+        check_cuda(cudaStreamSynchronize(h->stream), "phase_field_rhs");
+    });
+}
+
+int efsi_structure_tensor_rhs(efsi_handle* h, const double* sxx, const double* syy, const double* sxy,
+                              const double* U, const double* V, const double* phi, const double* G, double* rxx,
+                              double* ryy, double* rxy) {
+    return guarded(h, [&] {
+        DevBlock* d = h->dev;
+        k_reset_block<<<1, 1, 0, h->stream>>>(d);
+        h2d(h, h->Us, U, h->nu); h2d(h, h->Vs, V, h->nv); h2d(h, h->phis, phi, h->nc);
+        h2d(h, h->sxs, sxx, h->nc); h2d(h, h->sys, syy, h->nc); h2d(h, h->sxys, sxy, h->nc);
+        const double* Gp = nullptr;
+        if (G) { h2d(h, h->G, G, h->nc); Gp = h->G; }
+        StageFields f = stage_fields(h->Us, h->Vs, h->phis, h->c, h->sxs, h->sys, h->sxys, Gp);
+        launch_structure_rhs(h->P, f, h->Exx[0], h->Eyy[0], h->Exy[0], &d->st, h->stream);
+        fetch_dev(h);
+        raise_if_failed(h);
+        d2h(h, rxx, h->Exx[0], h->nc); d2h(h, ryy, h->Eyy[0], h->nc); d2h(h, rxy, h->Exy[0], h->nc);
+        check_cuda(cudaStreamSynchronize(h->stream), "structure_tensor_rhs");
+    });
+}
+
+int efsi_momentum_explicit_rhs(efsi_handle* h, double t, const double* U, const double* V, const double* phi,
+                               const double* sxx, const double* syy, const double* sxy, const double* G, double* Fx,
+                               double* Fy) {
+    return guarded(h, [&] {
+        DevBlock* d = h->dev;
+        k_reset_block<<<1, 1, 0, h->stream>>>(d);
+        h2d(h, h->Us, U, h->nu); h2d(h, h->Vs, V, h->nv); h2d(h, h->phis, phi, h->nc);
+        h2d(h, h->sxs, sxx, h->nc); h2d(h, h->sys, syy, h->nc); h2d(h, h->sxys, sxy, h->nc);
+        const double* Gp = nullptr;
+        if (G) { h2d(h, h->G, G, h->nc); Gp = h->G; }
+        StageFields f = stage_fields(h->Us, h->Vs, h->phis, h->c, h->sxs, h->sys, h->sxys, Gp);
+        const double* kappa = nullptr;
+        if (h->P.md.capillarity == EFSI_CAP_DIFFUSE_AREA) {
+            launch_capillary_curvature(h->P, f.phi, h->cap_a, h->cap_b, h->kappa, h->stream);
+            kappa = h->kappa;
+        }
+        // full-face outputs land in the predictor buffers
+        launch_momentum_full(h->P, t, f, kappa, h->pj.Up, h->pj.Vp, &d->st, h->stream);
+        fetch_dev(h);
+        raise_if_failed(h);
+        d2h(h, Fx, h->pj.Up, h->nu); d2h(h, Fy, h->pj.Vp, h->nv);
+        check_cuda(cudaStreamSynchronize(h->stream), "momentum_explicit_rhs");
+    });
+}
+
+int efsi_apply_viscous_operator(efsi_handle* h, const double* phi, const double* uv, double* out) {
+    return guarded(h, [&] {
+        if (!h->visc) throw Err{EFSI_ARG, "viscosity model is inactive"};
+        const int Nx = h->Nx, Ny = h->Ny;
+        // build full MAC arrays whose compact part is uv (boundary faces unused)
+        std::vector<double> Uf(h->nu, 0.0), Vf(h->nv, 0.0);
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                Uf[(size_t)i + (size_t)j * (Nx + 1)] = uv[(size_t)i + (size_t)j * Nx];
+                Vf[(size_t)i + (size_t)j * Nx] = uv[h->nc + (size_t)i + (size_t)j * Nx];
+            }
+        h2d(h, h->Us, Uf.data(), h->nu); h2d(h, h->Vs, Vf.data(), h->nv); h2d(h, h->phis, phi, h->nc);
+        launch_viscous_apply(h->P, h->Us, h->Vs, h->phis, h->Iu[0], h->Iv[0], h->stream);
+        d2h(h, out, h->Iu[0], h->nc);
+        d2h(h, out + h->nc, h->Iv[0], h->nc);
+        check_cuda(cudaStreamSynchronize(h->stream), "apply_viscous_operator");
+    });
+}
+
+int efsi_set_timed_site(efsi_handle* h, int32_t which) {
+    return guarded(h, [&] {
+        if (which < EFSI_SITE_NONE || which >= EFSI_SITE_COUNT) throw Err{EFSI_ARG, "unknown launch site"};
+        h->timed_site = which;
+        h->stats.site_launches = 0;
+        h->stats.site_ms = 0.0;
+        h->stats.site_bytes = 0.0;
+        h->site_used = 0;
+        h->site_bytes_pending = 0.0;
+    });
+}
+
+int efsi_get_stats(const efsi_handle* h, efsi_stats* s) {
+    if (!h || !s) return EFSI_ARG;
+    *s = h->stats;
+    return EFSI_OK;
+}
+
+}  // extern "C"

@@ -238,7 +238,9 @@ class Handle:
         return {"projection_iterations": list(s.projection_iterations),
                 "velocity_iterations": list(s.velocity_iterations),
                 "resource_iterations": list(s.resource_iterations),
-                "kernel_launches": int(s.kernel_launches)}
+                "kernel_launches": int(s.kernel_launches), "device_ms": float(s.device_ms),
+                "site_launches": int(s.site_launches), "site_ms": float(s.site_ms),
+                "site_bytes": float(s.site_bytes)}
 
 
 @dataclass
@@ -309,15 +311,18 @@ def make_velocity_compatible(state: FSIState, context: IMEXContext, work: IMEXWo
 def integrate_step(state: FSIState, t: float, dt: float, context: IMEXContext,
                    work: IMEXWorkspace) -> StepReport:
     """integrate_step! (TimeIntegrationIMEX.jl:1152-1256): advances `state` in place
-    from t to t+dt on the device and returns the StepReport."""
+    from t to t+dt on the device and returns the StepReport.  The workspace
+    correction (the projection warm start) travels with the state."""
     _validate_state(state, context.metrics)
     h = context.handle
-    h.set_correction(work.correction)
     arrs = [field64(a, s) for a, s in zip(state.arrays(), h.shapes())]
+    q = field64(work.correction, (context.metrics.Nx, context.metrics.Ny))
     rep = _abi.StepReportC()
-    h.call("integrate_step_host", *[_abi.dptr(a) for a in arrs], float(t), float(dt), C.byref(rep))
+    h.call("integrate_step_host", *[_abi.dptr(a) for a in arrs], _abi.dptr(q), float(t), float(dt),
+           C.byref(rep))
     for dst, src in zip(state.arrays(), arrs):
         if dst is not src:
             dst[...] = src
-    work.correction[...] = h.get_correction()
+    if q is not work.correction:
+        work.correction[...] = q
     return StepReport.from_c(rep)

@@ -28,6 +28,12 @@ extern "C" {
 
 #define EFSI_ABI_VERSION 1
 
+#if defined(__GNUC__)
+#define EFSI_API __attribute__((visibility("default")))
+#else
+#define EFSI_API
+#endif
+
 /* ---- status codes ------------------------------------------------------- */
 #define EFSI_OK            0
 #define EFSI_ARG           1  /* Julia ArgumentError (e.g. TimeIntegrationIMEX.jl:1121, Projection.jl:213) */
@@ -187,12 +193,36 @@ typedef struct efsi_projection_result {
     double compatibility_defect;
 } efsi_projection_result;
 
-/* Solver statistics of the most recent step or projection. */
+/* Kernel launch sites that efsi_set_timed_site() can bracket with CUDA events. */
+#define EFSI_SITE_NONE          (-1)
+#define EFSI_SITE_PHASE           0   /* phase-field right-hand side                     */
+#define EFSI_SITE_MOMENTUM        1   /* explicit momentum forcing                       */
+#define EFSI_SITE_STRUCTURE       2   /* structure-tensor right-hand side                */
+#define EFSI_SITE_VISC_APPLY      3   /* viscous operator history I_uv                   */
+#define EFSI_SITE_VISC_MATVEC     4   /* viscous CG: p update + (I - a A) p + p.Ap        */
+#define EFSI_SITE_VISC_UPDATE     5   /* viscous CG: x, r update + norms                 */
+#define EFSI_SITE_PCG_MATVEC      6   /* projection CG: p update + K p + p.Kp            */
+#define EFSI_SITE_PCG_UPDATE      7   /* projection CG: x, r update + |r|^2              */
+#define EFSI_SITE_VCYCLE          8   /* one multigrid V-cycle (all its kernels)         */
+#define EFSI_SITE_PROJ_RHS        9   /* predictor injection + Poisson right-hand side   */
+#define EFSI_SITE_PROJ_FINISH    10   /* correction, velocity update, diagnostics        */
+#define EFSI_SITE_COMBINE        11   /* stage combination of phi, sigma, c              */
+#define EFSI_SITE_VEL_RHS        12   /* viscous predictor right-hand side               */
+#define EFSI_SITE_FINALIZE       13   /* state commit + StepReport reductions            */
+#define EFSI_SITE_COUNT          14
+
+/* Solver statistics and device timings of the most recent call. */
 typedef struct efsi_stats {
     int32_t projection_iterations[4];   /* per stage; [0] = make_velocity_compatible      */
     int32_t velocity_iterations[4];     /* per stage (stages 2..4)                        */
     int32_t resource_iterations[4];
     int64_t kernel_launches;            /* kernels enqueued by the last call              */
+    double  device_ms;                  /* CUDA-event time of the last call on the handle's
+                                           stream (host<->device copies included)        */
+    int64_t site_launches;              /* timed-site launches since efsi_set_timed_site  */
+    double  site_ms;                    /* their summed CUDA-event duration               */
+    double  site_bytes;                 /* their summed algorithmic bytes (unique reads +
+                                           writes once, FP64)                            */
 } efsi_stats;
 
 typedef struct efsi_handle efsi_handle;
@@ -202,57 +232,59 @@ typedef struct efsi_handle efsi_handle;
  * supported viscous boundaries, Operators.jl:89-105), uploads boundary data and
  * allocates every device buffer on the current CUDA device.  On failure *out is
  * NULL and efsi_last_error(NULL) describes the cause. */
-int  efsi_create(const efsi_config* config, efsi_handle** out);
-void efsi_destroy(efsi_handle* handle);
+EFSI_API int  efsi_create(const efsi_config* config, efsi_handle** out);
+EFSI_API void efsi_destroy(efsi_handle* handle);
 /* Message of the last failing call on `handle` (NULL: last failing efsi_create
  * on this thread). */
-const char* efsi_last_error(const efsi_handle* handle);
+EFSI_API const char* efsi_last_error(const efsi_handle* handle);
 
 /* Copy a full FSIState (TimeIntegrationIMEX.jl:103-118) to / from the device. */
-int efsi_upload_state(efsi_handle* h, const double* U, const double* V, const double* phi,
+EFSI_API int efsi_upload_state(efsi_handle* h, const double* U, const double* V, const double* phi,
                       const double* resource, const double* sigma_xx,
                       const double* sigma_yy, const double* sigma_xy);
-int efsi_download_state(efsi_handle* h, double* U, double* V, double* phi, double* resource,
+EFSI_API int efsi_download_state(efsi_handle* h, double* U, double* V, double* phi, double* resource,
                         double* sigma_xx, double* sigma_yy, double* sigma_xy);
 
 /* IMEXWorkspace.correction, the projection warm start (TimeIntegrationIMEX.jl:386). */
-int efsi_set_correction(efsi_handle* h, const double* q);
-int efsi_get_correction(efsi_handle* h, double* q);
+EFSI_API int efsi_set_correction(efsi_handle* h, const double* q);
+EFSI_API int efsi_get_correction(efsi_handle* h, double* q);
 
 /* make_velocity_compatible! (TimeIntegrationIMEX.jl:1088-1109) on the device state. */
-int efsi_make_velocity_compatible(efsi_handle* h, efsi_projection_result* result);
+EFSI_API int efsi_make_velocity_compatible(efsi_handle* h, efsi_projection_result* result);
 
 /* integrate_step! (TimeIntegrationIMEX.jl:1152-1256) on the device-resident state. */
-int efsi_integrate_step(efsi_handle* h, double t, double dt, efsi_step_report* report);
+EFSI_API int efsi_integrate_step(efsi_handle* h, double t, double dt, efsi_step_report* report);
 
-/* integrate_step! as the drop-in sees it: the host FSIState arrays are uploaded,
- * advanced in place and downloaded (TimeIntegrationIMEX.jl:1152-1256, with the
- * state copies of :1169 and :1232-1238 crossing the host/device boundary). */
-int efsi_integrate_step_host(efsi_handle* h, double* U, double* V, double* phi,
+/* integrate_step! as the drop-in sees it: the host FSIState arrays and the
+ * workspace correction (the projection warm start) are uploaded, advanced in place
+ * and downloaded (TimeIntegrationIMEX.jl:1152-1256, with the state copies of :1169
+ * and :1232-1238 crossing the host/device boundary).  `correction` may be NULL to
+ * keep the device-resident warm start. */
+EFSI_API int efsi_integrate_step_host(efsi_handle* h, double* U, double* V, double* phi,
                              double* resource, double* sigma_xx, double* sigma_yy,
-                             double* sigma_xy, double t, double dt,
+                             double* sigma_xy, double* correction, double t, double dt,
                              efsi_step_report* report);
 
 /* n consecutive integrate_step! calls on the device-resident state with host
  * sync only at the end; t advances by dts[k].  reports may be NULL or hold n
  * entries.  On an error the state holds the last completed step and the
  * return value says which step failed (efsi_last_error). */
-int efsi_step_n(efsi_handle* h, double t0, const double* dts, int32_t n,
+EFSI_API int efsi_step_n(efsi_handle* h, double t0, const double* dts, int32_t n,
                 efsi_step_report* reports);
 
 /* Projection.project! (Projection.jl:170-307) of host velocity arrays onto
  * div(v) = target, using the context's correction boundaries and warm start. */
-int efsi_project(efsi_handle* h, double* U, double* V, const double* target,
+EFSI_API int efsi_project(efsi_handle* h, double* U, double* V, const double* target,
                  efsi_projection_result* result);
 
 /* phase_field_rhs for the context's phase-field method (PhaseFieldMethods.jl:408-475,
  * :652-671, :852-867) with target divergence G. */
-int efsi_phase_field_rhs(efsi_handle* h, const double* U, const double* V, const double* phi,
+EFSI_API int efsi_phase_field_rhs(efsi_handle* h, const double* U, const double* V, const double* phi,
                          const double* G, double* rhs);
 
 /* structure_tensor_rhs (StructureTensor.jl:377-463) with K_g built from G by the
  * context's growth-tensor model and the context's relaxation/extension. */
-int efsi_structure_tensor_rhs(efsi_handle* h, const double* sigma_xx, const double* sigma_yy,
+EFSI_API int efsi_structure_tensor_rhs(efsi_handle* h, const double* sigma_xx, const double* sigma_yy,
                               const double* sigma_xy, const double* U, const double* V,
                               const double* phi, const double* G,
                               double* rhs_xx, double* rhs_yy, double* rhs_xy);
@@ -260,7 +292,7 @@ int efsi_structure_tensor_rhs(efsi_handle* h, const double* sigma_xx, const doub
 /* Explicit momentum forcing of one stage (TimeIntegrationIMEX.jl:959-985):
  * -material_convection + body force + capillary force + div(phi tau_e)
  * + growth-viscous force, on the full MAC faces. */
-int efsi_momentum_explicit_rhs(efsi_handle* h, double t, const double* U, const double* V,
+EFSI_API int efsi_momentum_explicit_rhs(efsi_handle* h, double t, const double* U, const double* V,
                                const double* phi, const double* sigma_xx,
                                const double* sigma_yy, const double* sigma_xy,
                                const double* G, double* Fx, double* Fy);
@@ -268,10 +300,15 @@ int efsi_momentum_explicit_rhs(efsi_handle* h, double t, const double* U, const 
 /* apply_operator(build_viscous_operator(...), uv) (Operators.jl:929-1083, :1115)
  * on the compact velocity vector uv = [U(1:Nx,:); V(:,1:Ny)] with viscosity
  * evaluated from phi. */
-int efsi_apply_viscous_operator(efsi_handle* h, const double* phi, const double* uv,
+EFSI_API int efsi_apply_viscous_operator(efsi_handle* h, const double* phi, const double* uv,
                                 double* out);
 
-int efsi_get_stats(const efsi_handle* h, efsi_stats* stats);
+EFSI_API int efsi_get_stats(const efsi_handle* h, efsi_stats* stats);
+
+/* Bracket every launch of one EFSI_SITE_* with CUDA events on the handle's stream
+ * (EFSI_SITE_NONE switches timing off) and reset the site accumulators of
+ * efsi_stats.  Tracing aid of the benchmark; no reference counterpart. */
+EFSI_API int efsi_set_timed_site(efsi_handle* h, int32_t site);
 
 #ifdef __cplusplus
 }

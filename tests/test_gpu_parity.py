@@ -1,0 +1,333 @@
+"""Parity of the CUDA path (through the C-ABI) with the FP64 CPU oracle.
+
+Tolerances: explicit operators are pure FP64 stencils and must agree to 1e-12
+relative L2; full steps, with both sides' linear solves converged to 1e-13, must
+agree to 1e-10 relative L2 per field per step (and 1e-8 after many steps)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import eulerianfsi_b200 as ef
+from eulerianfsi_b200 import _abi, workloads
+from tests.gpu_util import pair, random_inputs, rel_err
+from tests.helpers import dp, fz, periodic_problem
+
+pytestmark = pytest.mark.gpu
+
+OP_TOL = 1e-12
+STEP_TOL = 1e-10
+TIGHT = dict(projection_reltol=1e-13, velocity_reltol=1e-13)
+
+
+def tight(numerics):
+    import dataclasses
+    ls = dataclasses.replace(numerics.linear_solvers, velocity_method="gmres", reltol=1e-13, maxiter=2000)
+    return dataclasses.replace(numerics, linear_solvers=ls, projection_reltol=1e-13, projection_maxiter=3000)
+
+
+def cavity_like(N, method, seed=0):
+    w = workloads.cavity_disk(N=N)
+    models = ef.FSIModels(viscosity=ef.ConstantViscosity(0.01), elastic_stress=ef.LinearInternalTensorStress(0.1),
+                          phase_field_method=method,
+                          growth_source=ef.ConstantIntrinsicGrowth(0.3), tensor_relaxation=ef.MaxwellRelaxation(0.5))
+    return w.metrics, w.bcs, models, tight(w.numerics)
+
+
+PF = {
+    "upwind": ef.NoPhaseFieldRegularization(),
+    "cdi": ef.CurrentCDIPhaseField(4.0, 2 / 24, delta_normal=1e-6),
+    "acdi": ef.JainACDIPhaseField(1.0, 0.51 / 24, delta_normal=1e-14, dynamic_gamma=False),
+    "acdi_dynamic": ef.JainACDIPhaseField(0.7, 0.51 / 24),
+    "uwcdi": ef.PirozzoliUWCDIPhaseField(1.0),
+    "uwcdi_youngs": ef.PirozzoliUWCDIPhaseField(1.0, normal_reconstruction="youngs"),
+    "uwcdi_smoothed9": ef.PirozzoliUWCDIPhaseField(1.0, normal_reconstruction="smoothed9"),
+}
+
+
+def _walls_consistent(inp, bcs_kind):
+    # zero normal velocity on walls so that Neumann inflow never occurs
+    inp["U"][0, :] = 0.0
+    inp["U"][-1, :] = 0.0
+    inp["V"][:, 0] = 0.0
+    inp["V"][:, -1] = 0.0
+    return inp
+
+
+@pytest.mark.parametrize("name", list(PF))
+@pytest.mark.parametrize("periodic", [False, True])
+def test_phase_field_rhs(name, periodic):
+    N = 40
+    if periodic:
+        grid, metrics, bcs, models = periodic_problem(N, PF[name])
+        numerics = ef.IMEXNumerics()
+    else:
+        metrics, bcs, models, numerics = cavity_like(N, PF[name])
+    gpu, ora = pair(metrics, bcs, models, numerics)
+    inp = random_inputs(metrics, seed=3)
+    if not periodic:
+        _walls_consistent(inp, "cavity")
+    else:
+        inp["U"][-1, :] = inp["U"][0, :]
+        inp["V"][:, -1] = inp["V"][:, 0]
+    outs = []
+    for h in (gpu, ora):
+        r = fz(N, N)
+        h.call("phase_field_rhs", dp(inp["U"]), dp(inp["V"]), dp(inp["phi"]), dp(inp["G"]), dp(r))
+        outs.append(r)
+    assert rel_err(outs[0], outs[1]) <= OP_TOL, rel_err(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("periodic", [False, True])
+def test_structure_tensor_rhs(periodic):
+    N = 36
+    if periodic:
+        grid, metrics, bcs, models = periodic_problem(N, ef.NoPhaseFieldRegularization(),
+                                                      tensor_relaxation=ef.MaxwellRelaxation(0.3),
+                                                      growth_source=ef.ConstantIntrinsicGrowth(0.2),
+                                                      growth_tensor=ef.DirectionalGrowthTensor(1.0, 2.0))
+        numerics = ef.IMEXNumerics(structure_extension=ef.GeometricStructureExtension(20.0, 4.0))
+    else:
+        metrics, bcs, models, numerics = cavity_like(N, ef.NoPhaseFieldRegularization())
+    gpu, ora = pair(metrics, bcs, models, numerics)
+    inp = random_inputs(metrics, seed=5)
+    if not periodic:
+        _walls_consistent(inp, "cavity")
+    outs = []
+    for h in (gpu, ora):
+        r = [fz(N, N) for _ in range(3)]
+        h.call("structure_tensor_rhs", dp(inp["sxx"]), dp(inp["syy"]), dp(inp["sxy"]), dp(inp["U"]), dp(inp["V"]),
+               dp(inp["phi"]), dp(inp["G"]), *[dp(a) for a in r])
+        outs.append(r)
+    for a, b in zip(*outs):
+        assert rel_err(a, b) <= OP_TOL, rel_err(a, b)
+
+
+@pytest.mark.parametrize("case", ["cavity", "periodic", "filament", "capillary"])
+def test_momentum_explicit_rhs(case):
+    N = 32
+    if case == "cavity":
+        metrics, bcs, models, numerics = cavity_like(N, ef.NoPhaseFieldRegularization())
+    elif case == "periodic":
+        grid, metrics, bcs, models = periodic_problem(N, None, viscosity=ef.HarmonicPhaseViscosity(0.01, 0.1),
+                                                      elastic_stress=ef.LinearInternalTensorStress(0.4),
+                                                      growth_source=ef.ConstantIntrinsicGrowth(0.2),
+                                                      body_force=ef.ConstantBodyForce(0.1, -0.2))
+        numerics = ef.IMEXNumerics()
+    elif case == "filament":
+        w = workloads.filament_kolmogorov(N=N)
+        metrics, bcs, models, numerics = w.metrics, w.bcs, w.models, w.numerics
+    else:
+        w = workloads.cavity_disk(N=N)
+        models = ef.FSIModels(viscosity=ef.ConstantViscosity(0.01), elastic_stress=ef.LinearInternalTensorStress(0.1),
+                              capillarity=ef.DiffuseAreaCapillarity(0.05, smoothing_passes=2),
+                              phase_field_method=ef.NoPhaseFieldRegularization())
+        metrics, bcs, numerics = w.metrics, w.bcs, w.numerics
+    gpu, ora = pair(metrics, bcs, models, numerics)
+    inp = random_inputs(metrics, seed=7)
+    outs = []
+    for h in (gpu, ora):
+        Fx, Fy = fz(N + 1, N), fz(N, N + 1)
+        h.call("momentum_explicit_rhs", 0.3, dp(inp["U"]), dp(inp["V"]), dp(inp["phi"]), dp(inp["sxx"]),
+               dp(inp["syy"]), dp(inp["sxy"]), dp(inp["G"]), dp(Fx), dp(Fy))
+        outs.append((Fx, Fy))
+    for a, b in zip(*outs):
+        assert rel_err(a, b) <= OP_TOL, rel_err(a, b)
+
+
+@pytest.mark.parametrize("case", ["cavity", "periodic_harmonic", "filament"])
+def test_viscous_operator(case):
+    N = 28
+    if case == "cavity":
+        metrics, bcs, models, numerics = cavity_like(N, ef.NoPhaseFieldRegularization())
+    elif case == "periodic_harmonic":
+        grid, metrics, bcs, models = periodic_problem(N, None, viscosity=ef.HarmonicPhaseViscosity(0.01, 0.2))
+        numerics = ef.IMEXNumerics()
+    else:
+        w = workloads.filament_kolmogorov(N=N)
+        metrics, bcs, models, numerics = w.metrics, w.bcs, w.models, w.numerics
+    gpu, ora = pair(metrics, bcs, models, numerics)
+    inp = random_inputs(metrics, seed=11)
+    uv = np.concatenate([inp["U"][:N, :].ravel(order="F"), inp["V"][:, :N].ravel(order="F")])
+    outs = []
+    for h in (gpu, ora):
+        o = np.zeros(2 * N * N)
+        h.call("apply_viscous_operator", dp(inp["phi"]), dp(uv), dp(o))
+        outs.append(o)
+    assert rel_err(outs[0], outs[1]) <= OP_TOL
+
+
+@pytest.mark.parametrize("case", ["cavity_neumann", "dirichlet", "periodic", "channel"])
+def test_projection(case):
+    if case == "cavity_neumann":
+        w = workloads.cavity_disk(N=48)
+        metrics, bcs, models, numerics = w.metrics, w.bcs, w.models, tight(w.numerics)
+    elif case == "periodic":
+        grid, metrics, bcs, models = periodic_problem(64, None)
+        numerics = ef.IMEXNumerics(projection_reltol=1e-13)
+    elif case == "channel":
+        w = workloads.channel_growth(N=32)
+        metrics, bcs, models, numerics = w.metrics, w.bcs, w.models, tight(w.numerics)
+    else:
+        grid = ef.generate_grid(1.0, 1.0, 40, 40)
+        metrics = ef.build_mesh_metrics(grid)
+        d0, n0 = ef.Dirichlet(0.0), ef.Neumann(0.0)
+        bq = ef.BoundaryConditionSetup(d0, d0, d0, d0)
+        nb = ef.BoundaryConditionSetup(n0, n0, n0, n0)
+        bcs = ef.FSIBoundaryConditions(nb, nb, bq, nb, {"xx": nb, "yy": nb, "xy": nb})
+        models, numerics = ef.FSIModels(), ef.IMEXNumerics(projection_reltol=1e-13)
+    gpu, ora = pair(metrics, bcs, models, numerics)
+    inp = random_inputs(metrics, seed=13)
+    Nx, Ny = metrics.Nx, metrics.Ny
+    G = inp["G"] if case in ("dirichlet", "channel") else fz(Nx, Ny)
+    if case == "periodic":
+        inp["U"][-1, :] = inp["U"][0, :]
+        inp["V"][:, -1] = inp["V"][:, 0]
+    if case == "cavity_neumann":  # compatible: zero boundary flux, zero target
+        inp["U"][0, :] = inp["U"][-1, :] = 0.0
+        inp["V"][:, 0] = inp["V"][:, -1] = 0.0
+    res = []
+    for h in (gpu, ora):
+        U, V = inp["U"].copy(order="F"), inp["V"].copy(order="F")
+        h.set_correction(fz(Nx, Ny))
+        r = _abi.ProjectionResultC()
+        h.call("project", dp(U), dp(V), dp(G), C.byref(r))
+        res.append((U, V, h.get_correction(), r))
+    (U1, V1, q1, r1), (U2, V2, q2, r2) = res
+    assert rel_err(U1, U2) <= 1e-10 and rel_err(V1, V2) <= 1e-10
+    assert rel_err(q1, q2) <= 1e-10
+    assert r1.constraint_linf <= 1e-9 and r2.constraint_linf <= 1e-9
+
+
+def test_projection_incompatible_source_raises():
+    grid, metrics, bcs, models = periodic_problem(8, None)
+    gpu, _ = pair(metrics, bcs, models, ef.IMEXNumerics())
+    r = _abi.ProjectionResultC()
+    with pytest.raises(ef.ArgumentError):
+        gpu.call("project", dp(fz(9, 8)), dp(fz(8, 9)), dp(np.full((8, 8), 0.1, order="F")), C.byref(r))
+
+
+def _run_steps(w, steps, compatible=False):
+    gpu, ora = pair(w.metrics, w.bcs, w.models, tight(w.numerics))
+    states = []
+    reps = []
+    for h in (gpu, ora):
+        st = w.state.copy()
+        h.upload(st)
+        h.set_correction(fz(w.metrics.Nx, w.metrics.Ny))
+        if compatible:
+            r = _abi.ProjectionResultC()
+            h.call("make_velocity_compatible", C.byref(r))
+        t = 0.0
+        rr = []
+        for k in range(steps):
+            rep = _abi.StepReportC()
+            h.call("integrate_step", t, w.dt, C.byref(rep))
+            rr.append(ef.StepReport.from_c(rep))
+            t += w.dt
+        h.download(st)
+        states.append(st)
+        reps.append(rr)
+    return states, reps, gpu
+
+
+def _assert_states(a, b, tol):
+    for name in ("U", "V", "phi", "resource", "sigma_xx", "sigma_yy", "sigma_xy"):
+        e = rel_err(getattr(a, name), getattr(b, name))
+        assert e <= tol, (name, e)
+
+
+@pytest.mark.parametrize("N", [16, 32])
+def test_cavity_disk_one_step(N):
+    w = workloads.cavity_disk(N=N)
+    (g, o), (rg, ro), _ = _run_steps(w, 1)
+    _assert_states(g, o, STEP_TOL)
+    assert abs(rg[0].minimum_phi - ro[0].minimum_phi) <= 1e-12
+    assert abs(rg[0].minimum_sigma_eigenvalue - ro[0].minimum_sigma_eigenvalue) <= 1e-10
+
+
+def test_cavity_disk_many_steps():
+    w = workloads.cavity_disk(N=32)
+    (g, o), _, _ = _run_steps(w, 30)
+    _assert_states(g, o, 1e-8)
+
+
+def test_filament_steps():
+    w = workloads.filament_kolmogorov(N=32)
+    (g, o), _, _ = _run_steps(w, 5)
+    _assert_states(g, o, STEP_TOL * 10)
+
+
+def test_channel_growth_steps():
+    w = workloads.channel_growth(N=16)
+    (g, o), (rg, ro), _ = _run_steps(w, 3, compatible=True)
+    _assert_states(g, o, STEP_TOL * 10)
+    assert rg[-1].minimum_resource > 0
+
+
+def test_reference_growth_smoke_on_gpu():
+    """test/growth_tests.jl:96-142 through the CUDA library."""
+    from tests.test_oracle_known_answers import growth_smoke_problem
+    grid, metrics, bcs, models, state = growth_smoke_problem()
+    ctx = ef.build_imex_context(metrics, bcs, models, use_projection_amg=False)
+    work = ef.allocate_imex_workspace(metrics)
+    res = ef.make_velocity_compatible(state, ctx, work)
+    assert res.constraint_linf < 1e-7
+    assert np.max(np.abs(state.U)) > 0.0
+    work.correction[...] = 0.0
+    rep = ef.integrate_step(state, 0.0, 1e-4, ctx, work)
+    assert rep.maximum_projection_constraint_linf < 1e-6
+    assert np.max(np.abs(state.U[-1, :] - state.U[0, :])) < 1e-12
+    assert np.max(np.abs(state.V[:, -1])) < 1e-12
+    assert rep.maximum_growth_trace_error < 1e-12
+    assert rep.minimum_resource > 0.0
+    assert np.all(np.isfinite(state.phi)) and np.all(np.isfinite(state.sigma_xx))
+
+
+def test_reference_rest_state_on_gpu():
+    """test/growth_tests.jl:144-162 through the CUDA library."""
+    grid, metrics, bcs, models = periodic_problem(8, None)
+    state = ef.FSIState(fz(9, 8), fz(8, 9), np.full((8, 8), 0.5), np.ones((8, 8)), np.ones((8, 8)), fz(8, 8))
+    ctx = ef.build_imex_context(metrics, bcs, models, use_projection_amg=False)
+    work = ef.allocate_imex_workspace(metrics)
+    ef.make_velocity_compatible(state, ctx, work)
+    rep = ef.integrate_step(state, 0.0, 1e-4, ctx, work)
+    assert rep.maximum_growth_trace_error == 0.0
+    assert np.all(state.resource == 0.0)
+    assert np.max(np.abs(state.U)) < 1e-9 and np.max(np.abs(state.V)) < 1e-9
+    assert np.max(np.abs(state.phi - 0.5)) < 1e-9
+
+
+def test_stage1_constraint_violation_raises_and_keeps_state():
+    w = workloads.cavity_disk(N=16)
+    ctx = ef.build_imex_context(w.metrics, w.bcs, w.models, numerics=w.numerics)
+    work = ef.allocate_imex_workspace(w.metrics)
+    st = w.state.copy()
+    st.U[5, 5] = 0.5  # divergent velocity entering stage 1
+    before = st.copy()
+    with pytest.raises(ef.ArgumentError):
+        ef.integrate_step(st, 0.0, w.dt, ctx, work)
+    np.testing.assert_array_equal(st.U, before.U)
+
+
+def test_nonfinite_state_raises():
+    w = workloads.cavity_disk(N=16)
+    ctx = ef.build_imex_context(w.metrics, w.bcs, w.models, numerics=w.numerics)
+    work = ef.allocate_imex_workspace(w.metrics)
+    st = w.state.copy()
+    st.phi[3, 3] = np.nan
+    with pytest.raises(ef.ArgumentError):
+        ef.integrate_step(st, 0.0, w.dt, ctx, work)
+
+
+def test_phase_mass_conservation():
+    w = workloads.cavity_disk(N=32)
+    ctx = ef.build_imex_context(w.metrics, w.bcs, w.models, numerics=w.numerics)
+    work = ef.allocate_imex_workspace(w.metrics)
+    st = w.state.copy()
+    m0 = st.phi.sum()
+    t = 0.0
+    for _ in range(10):
+        ef.integrate_step(st, t, w.dt, ctx, work)
+        t += w.dt
+    assert abs(st.phi.sum() - m0) / m0 <= 1e-12
