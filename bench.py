@@ -172,14 +172,16 @@ def run_ours(args, rank, world, local_rank):
     if args.warmup:
         h.call("step_n", t, dts, int(args.warmup), None)
         t += args.warmup * w.dt
-    site = _abi.SITES.index(args.site)
-    h.call("set_timed_site", site)
+    h.call("set_timed_site", -1)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local_rank) as clocks:
         h.call("step_n", t, dts, int(args.steps), None)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t += args.steps * w.dt
     st = h.stats()
     ms = st["device_ms"]
     launches = st["kernel_launches"]
@@ -188,13 +190,21 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
     value = world * w.cells * args.steps / (ms / 1e3)
+
+    # ---- roofline of one kernel: the same steps enqueued from the host with CUDA events
+    # around every launch of the site (per-launch events cannot sit inside graph loops)
     peak, peak_kind = _peaks()
-    site_ms = st["site_ms"] / max(st["site_launches"], 1)
-    site_bytes = st["site_bytes"] / max(st["site_launches"], 1)
+    site_steps = max(1, min(args.site_steps, args.steps))
+    h.call("set_timed_site", _abi.SITES.index(args.site))
+    h.call("step_n", t, dts, site_steps, None)
+    t += site_steps * w.dt
+    sst = h.stats()
+    h.call("set_timed_site", -1)
+    site_ms = sst["site_ms"] / max(sst["site_launches"], 1)
+    site_bytes = sst["site_bytes"] / max(sst["site_launches"], 1)
     achieved = site_bytes / (site_ms / 1e3) / 1e9 if site_ms > 0 else None
 
     # ---- end to end through the public API with pinned host arrays ----
-    h.call("set_timed_site", -1)
     e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, args.e2e_steps))
     pinned = []
     for a in w.state.arrays():
@@ -234,7 +244,8 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "kernel": args.site, "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": args.traffic,
-                     "avg_launch_us": site_ms * 1e3, "algorithmic_bytes_per_launch": site_bytes},
+                     "avg_launch_us": site_ms * 1e3, "algorithmic_bytes_per_launch": site_bytes,
+                     "launches_timed": sst["site_launches"], "site_steps": site_steps},
         "clocks": clocks.summary(),
         "solver": {"projection_iterations": st["projection_iterations"],
                    "velocity_iterations": st["velocity_iterations"]},
@@ -259,6 +270,7 @@ def main():
     p.add_argument("--velocity-reltol", type=float, default=1e-8)
     p.add_argument("--site", default="pcg_update")
     p.add_argument("--traffic", type=float, default=None, help="ncu dram bytes per launch of the site")
+    p.add_argument("--site-steps", type=int, default=3)
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--cpu-steps", type=int, default=1)
     p.add_argument("--cpu-budget", type=float, default=60.0)

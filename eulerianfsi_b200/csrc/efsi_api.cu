@@ -2,15 +2,20 @@
 // device buffers, the four-stage orchestration of TimeIntegrationIMEX.jl:1152-1256
 // and the operator-level entry points.
 //
-// Orchestration: one CUDA stream per handle.  Every kernel of a step is enqueued
-// back to back; the Krylov solves keep their scalars on the device and are
-// enqueued in batches sized from the previous solve's iteration count, so a step
-// synchronises with the host only a few times.  Device-side errors (the Julia
-// exceptions of the reference) are raised into a status word and reported after
-// the step; a failing step leaves the state untouched.
+// Orchestration: one CUDA stream per handle.  The whole step is captured once as a
+// CUDA graph; every Krylov solve keeps its scalars on the device and becomes a
+// conditional WHILE node whose body (two iterations) clears the loop flag when the
+// residual test passes, so a step is one graph launch and a batch of steps needs
+// one host synchronisation.  (t, dt) come from a device array indexed by a step
+// counter, so the same graph serves every step.  When a launch site is being timed
+// (or EFSI_STEP_GRAPH=0) the step is enqueued from the host instead, with the solves
+// in batches sized from the previous solve's iteration count.  Device-side errors
+// (the Julia exceptions of the reference) are raised into a status word and
+// reported after the step; a failing step leaves the state untouched.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -32,7 +37,19 @@ struct DevBlock {
     double max_constraint;
     double max_trace;
     double gamma_dyn;
+    double t, dt;         // current step (read by the kernels: a captured graph serves every dt)
+    int counter;          // steps completed in the current batch
+    int first_fail;       // batch index of the first failing step, -1 if none
+    int iters[3][4];      // CG iterations of the current step: [projection|velocity|resource][stage]
 };
+
+// Per-step record written on the device at the end of every step.
+struct StepRec {
+    double v[7];          // StepReport (constraint, trace, min/max phi, min c, min eig, |det-1|)
+    long long nonspd;
+    int iters[3][4];
+};
+constexpr int kMaxBatch = 1024;  // steps per device batch (efsi_step_n is chunked)
 
 struct Err {
     int code;
@@ -79,9 +96,21 @@ struct efsi_handle {
     DevBlock* host = nullptr;  // pinned mirror
     int* done_pinned = nullptr;
     RedSlot slot[8];
-    // solver batch predictions
-    int pred_proj = 4, pred_visc = 4, pred_diff = 4;
+    // solver batch predictions (host-driven mode)
+    int pred[3] = {4, 4, 4};
     long long launches = 0;
+    // step graph: the whole IMEX step captured once, CG loops as WHILE nodes
+    cudaStream_t stream2 = nullptr;
+    bool use_graph = true, capturing = false;
+    cudaGraph_t step_graph = nullptr;
+    cudaGraphExec_t step_exec = nullptr;
+    long long fixed_launches = 0;
+    struct Loop { int kind, stage, kernels_per_body, iters_per_body; };
+    std::vector<Loop> loops;
+    double* times_dev = nullptr;    // (t, dt) per step of a batch
+    double* times_pinned = nullptr;
+    StepRec* hist_dev = nullptr;
+    StepRec* hist_pinned = nullptr;
     // CUDA-event timing: whole calls and one selectable launch site
     cudaEvent_t call_ev[2] = {nullptr, nullptr};
     int timed_site = EFSI_SITE_NONE;
@@ -103,8 +132,13 @@ struct efsi_handle {
         for (auto& e : site_ev) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
         for (cudaEvent_t e : call_ev) if (e) cudaEventDestroy(e);
         for (void* p : allocs) cudaFree(p);
+        if (step_exec) cudaGraphExecDestroy(step_exec);
+        if (step_graph) cudaGraphDestroy(step_graph);
         if (host) cudaFreeHost(host);
         if (done_pinned) cudaFreeHost(done_pinned);
+        if (times_pinned) cudaFreeHost(times_pinned);
+        if (hist_pinned) cudaFreeHost(hist_pinned);
+        if (stream2) cudaStreamDestroy(stream2);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -127,7 +161,7 @@ void reset_call_stats(efsi_handle* h) {
 // Bracket a launch site with CUDA events when it is the timed one.
 template <class F>
 void site(efsi_handle* h, int which, double bytes, F&& f) {
-    if (h->timed_site != which) { f(); return; }
+    if (h->capturing || h->timed_site != which) { f(); return; }
     if (h->site_used == h->site_ev.size()) {
         cudaEvent_t a, b;
         check_cuda(cudaEventCreate(&a), "event");
@@ -495,40 +529,87 @@ void raise_if_failed(efsi_handle* h) {
     }
 }
 
-// Zero the per-call scalars (status, maxima).
-__global__ void k_reset_block(DevBlock* d) {
+// ---------------------------------------------------------------------------------------
+// per-call / per-step device bookkeeping
+// ---------------------------------------------------------------------------------------
+__global__ void k_reset_call(DevBlock* d) {  // status and batch counters
     d->st.code = 0;
+    d->counter = 0;
+    d->first_fail = -1;
     d->max_constraint = 0.0;
     d->max_trace = 0.0;
 }
+__global__ void k_begin_step(DevBlock* d, const double* __restrict__ times) {
+    const int c = d->counter;
+    d->t = times[2 * c];
+    d->dt = times[2 * c + 1];
+    d->max_constraint = 0.0;
+    d->max_trace = 0.0;
+    for (int k = 0; k < 12; ++k) (&d->iters[0][0])[k] = 0;
+}
+__global__ void k_end_step(DevBlock* d, StepRec* hist) {
+    StepRec& r = hist[d->counter];
+    r.v[0] = d->max_constraint;
+    r.v[1] = d->max_trace;
+    for (int k = 0; k < 5; ++k) r.v[2 + k] = d->report[k];
+    r.nonspd = d->nonspd;
+    for (int k = 0; k < 12; ++k) (&r.iters[0][0])[k] = (&d->iters[0][0])[k];
+    if (d->st.code != 0 && d->first_fail < 0) d->first_fail = d->counter;
+    d->counter += 1;
+}
 
 // ---------------------------------------------------------------------------------------
-// CG drivers: enqueue predicted iterations, then confirm `done` on the host
+// CG solves: captured as a WHILE node, or driven from the host in predicted batches
 // ---------------------------------------------------------------------------------------
-template <class Iter>
-int run_cg(efsi_handle* h, CGScal* cg, int maxiter, int& pred, Iter&& iter, int kernels_per_iter, int where) {
-    int it = 0;
-    int batch = std::max(1, std::min(pred, maxiter));
+enum { KIND_PROJ = 0, KIND_VISC = 1, KIND_DIFF = 2 };
+
+template <class Init, class Body>
+void solve(efsi_handle* h, int kind, int stage, CGScal* cg, int maxiter, int kernels_per_body, int iters_per_body,
+           Init&& init, Body&& body) {
+    int* iters_out = &h->dev->iters[kind][stage];
+    if (h->capturing) {
+        cudaGraph_t g;
+        cudaStreamCaptureStatus cs;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        check_cuda(cudaStreamGetCaptureInfo(h->stream, &cs, nullptr, &g, &deps, &nd), "capture info");
+        cudaGraphConditionalHandle ch;
+        check_cuda(cudaGraphConditionalHandleCreate(&ch, g, 1, cudaGraphCondAssignDefault), "conditional handle");
+        init(h->stream, iters_out, ch);
+        check_cuda(cudaStreamGetCaptureInfo(h->stream, &cs, nullptr, &g, &deps, &nd), "capture info");
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = ch;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        check_cuda(cudaGraphAddNode(&node, g, deps, nd, &np), "conditional node");
+        check_cuda(cudaStreamUpdateCaptureDependencies(h->stream, &node, 1, cudaStreamSetCaptureDependencies),
+                   "capture dependencies");
+        cudaGraph_t bg = np.conditional.phGraph_out[0];
+        check_cuda(cudaStreamBeginCaptureToGraph(h->stream2, bg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed),
+                   "body capture");
+        body(h->stream2, iters_out, ch);
+        cudaGraph_t out;
+        check_cuda(cudaStreamEndCapture(h->stream2, &out), "body capture");
+        h->loops.push_back({kind, stage, kernels_per_body, iters_per_body});
+        return;
+    }
+    init(h->stream, iters_out, (cudaGraphConditionalHandle)0);
+    int bodies = 0;
+    int batch = std::max(1, (h->pred[kind] + iters_per_body - 1) / iters_per_body);
     int* flags = h->done_pinned;  // iter, done, maxiter, conv (CGScal order)
     while (true) {
-        int k = 0;
-        for (; k < batch && it < maxiter; ++k, ++it) iter(it);
-        h->launches += (long long)k * kernels_per_iter;
+        for (int k = 0; k < batch && bodies * iters_per_body < maxiter; ++k, ++bodies)
+            body(h->stream, iters_out, (cudaGraphConditionalHandle)0);
+        h->launches += (long long)batch * kernels_per_body;
         check_cuda(cudaMemcpyAsync(flags, &cg->iter, 4 * sizeof(int), cudaMemcpyDeviceToHost, h->stream),
                    "cg readback");
         check_cuda(cudaStreamSynchronize(h->stream), "cg");
-        if (flags[1] || it >= maxiter) break;
-        batch = 2;
+        if (flags[1] || bodies * iters_per_body >= maxiter) break;
+        batch = 1;
     }
-    const int iters = flags[0], conv = flags[3];
-    pred = std::max(1, iters);
-    (void)where;
-    return conv ? iters : -iters;
-}
-
-StageFields stage_fields(const double* U, const double* V, const double* phi, const double* c, const double* sxx,
-                         const double* syy, const double* sxy, const double* G) {
-    return StageFields{U, V, phi, c, sxx, syy, sxy, G};
+    h->pred[kind] = std::max(1, flags[0]);
 }
 
 // Algorithmic bytes (unique FP64 reads + writes once) of one V-cycle.
@@ -542,6 +623,8 @@ double vcycle_bytes(const Projection& pj) {
     return 8.0 * (b + nc * nc + 2.0 * nc);
 }
 
+int vcycle_kernels(const Projection& pj) { return 5 * (pj.nlev - 1) + 1 + (pj.nlev == 1 ? 1 : 0); }
+
 // One projection of (compact predictor | full arrays) onto div = G, writing U_out/V_out/q.
 void projection(efsi_handle* h, bool compact, const double* u_in, const double* v_in, const double* G, double* U_out,
                 double* V_out, int stage_slot) {
@@ -550,21 +633,24 @@ void projection(efsi_handle* h, bool compact, const double* u_in, const double* 
     const double N = (double)h->nc, nuv = (double)(h->nu + h->nv), g = G ? 1.0 : 0.0;
     site(h, EFSI_SITE_PROJ_RHS, 8.0 * (2.0 * nuv + N * (2.0 + g)),
          [&] { proj_rhs(P, h->pj, compact, u_in, v_in, G, &d->ps, h->slot[0], &d->st, h->stream); });
-    proj_cg_init(P, h->pj, P.nu.projection_reltol, P.nu.projection_maxiter, h->q, &d->cg_proj, &d->ps, h->slot[1],
-                 h->slot[2], &d->st, h->stream);
-    h->launches += 2 + 6 * (h->pj.nlev - 1) + 1;
     const double vb = vcycle_bytes(h->pj);
-    int iters = run_cg(
-        h, &d->cg_proj, P.nu.projection_maxiter, h->pred_proj,
-        [&](int it) {
-            site(h, EFSI_SITE_PCG_MATVEC, 8.0 * N * (it == 0 ? 3.0 : 4.0),
-                 [&] { proj_matvec(P, h->pj, it, &d->cg_proj, h->slot[3], h->stream); });
-            site(h, EFSI_SITE_PCG_UPDATE, 8.0 * N * 6.0,
-                 [&] { proj_update(P, h->pj, it, &d->cg_proj, h->slot[4], h->stream); });
-            site(h, EFSI_SITE_VCYCLE, vb, [&] { proj_vcycle(P, h->pj, &d->cg_proj, h->slot[5], h->stream); });
+    const int vk = vcycle_kernels(h->pj);
+    solve(
+        h, KIND_PROJ, stage_slot, &d->cg_proj, P.nu.projection_maxiter, 2 * (2 + vk), 2,
+        [&](cudaStream_t s, int* io, cudaGraphConditionalHandle ch) {
+            proj_cg_init(P, h->pj, P.nu.projection_reltol, P.nu.projection_maxiter, h->q, &d->cg_proj, &d->ps,
+                         h->slot[1], h->slot[2], &d->st, io, ch, s);
+            h->launches += 1 + vk;
         },
-        proj_kernels_per_iter(h->pj), 2);
-    h->stats.projection_iterations[stage_slot] = std::abs(iters);
+        [&](cudaStream_t s, int* io, cudaGraphConditionalHandle ch) {
+            for (int par = 0; par < 2; ++par) {
+                site(h, EFSI_SITE_PCG_MATVEC, 8.0 * N * 4.0,
+                     [&] { proj_matvec(P, h->pj, par, &d->cg_proj, h->slot[3], s); });
+                site(h, EFSI_SITE_PCG_UPDATE, 8.0 * N * 6.0,
+                     [&] { proj_update(P, h->pj, par, &d->cg_proj, h->slot[4], io, ch, s); });
+                site(h, EFSI_SITE_VCYCLE, vb, [&] { proj_vcycle(P, h->pj, &d->cg_proj, h->slot[5], s); });
+            }
+        });
     site(h, EFSI_SITE_PROJ_FINISH, 8.0 * (4.0 * N + 2.0 * nuv + g * N), [&] {
         proj_finish(P, h->pj, G, h->q, U_out, V_out, &d->ps, &d->max_constraint, h->slot[6], h->slot[7], &d->st,
                     h->stream);
@@ -572,7 +658,7 @@ void projection(efsi_handle* h, bool compact, const double* u_in, const double* 
     h->launches += 3;
 }
 
-void tendencies(efsi_handle* h, int s, double t_stage, const StageFields& f) {
+void tendencies(efsi_handle* h, int s, const StageFields& f) {
     const Params& P = h->P;
     DevBlock* d = h->dev;
     const double N = (double)h->nc, nuv = (double)(h->nu + h->nv), g = f.G ? 1.0 : 0.0;
@@ -582,8 +668,9 @@ void tendencies(efsi_handle* h, int s, double t_stage, const StageFields& f) {
         kappa = h->kappa;
         h->launches += 1 + P.md.capillary_smoothing_passes;
     }
+    // the supported body forces are steady, so the stage time does not enter the kernels
     site(h, EFSI_SITE_MOMENTUM, 8.0 * (nuv + N * (4.0 + g) + 2.0 * N),
-         [&] { launch_momentum_rhs(P, t_stage, f, kappa, h->Eu[s], h->Ev[s], &d->st, h->stream); });
+         [&] { launch_momentum_rhs(P, 0.0, f, kappa, h->Eu[s], h->Ev[s], &d->st, h->stream); });
     if (P.md.phase_field_method == EFSI_PF_ACDI && P.md.pf_option) {
         launch_umax(P, f.U, f.V, &d->gamma_dyn, h->slot[0], h->stream);
         h->launches += 1;
@@ -600,28 +687,28 @@ void tendencies(efsi_handle* h, int s, double t_stage, const StageFields& f) {
 }
 
 const double c_AI_diag[4] = {0.0, 4.0 / 15, 1.0 / 15, 1.0 / 6};
-const double c_CS[4] = {0.0, 8.0 / 15, 2.0 / 3, 1.0};
 
-void enqueue_step(efsi_handle* h, double t, double dt) {
+// The whole IMEX step (TimeIntegrationIMEX.jl:1159-1255) for the (t, dt) at the
+// batch counter; identical for every step so that it can be captured once.
+void enqueue_step(efsi_handle* h) {
     const Params& P = h->P;
     DevBlock* d = h->dev;
     cudaStream_t s = h->stream;
-    std::memset(h->stats.projection_iterations, 0, sizeof(h->stats.projection_iterations));
-    std::memset(h->stats.velocity_iterations, 0, sizeof(h->stats.velocity_iterations));
-    std::memset(h->stats.resource_iterations, 0, sizeof(h->stats.resource_iterations));
-    k_reset_block<<<1, 1, 0, s>>>(d);
+    const double* dtp = &d->dt;
+    k_begin_step<<<1, 1, 0, s>>>(d, h->times_dev);
     launch_prepare_step(P, h->U, h->V, h->phi, h->c, h->sxx, h->syy, h->sxy, h->sxn, h->syn, h->sxyn, &d->st, s);
     h->launches += 2;
     const double* Gp = h->growth ? h->G : nullptr;
+    const double N = (double)h->nc;
     for (int st = 0; st < 4; ++st) {
         StageFields f;
         if (st == 0) {
-            f = stage_fields(h->U, h->V, h->phi, h->c, h->sxn, h->syn, h->sxyn, Gp);
+            f = StageFields{h->U, h->V, h->phi, h->c, h->sxn, h->syn, h->sxyn, Gp};
         } else {
             bool rc = h->resource;
             const double nE = (st == 1) ? 1.0 : 2.0;
-            site(h, EFSI_SITE_COMBINE, 8.0 * (double)h->nc * (4.0 + 4.0 * nE + 4.0 + (rc ? 2.0 + 2.0 * st : 0.0)), [&] {
-                launch_combine_scalars(P, st, dt, h->phi, h->sxn, h->syn, h->sxyn, h->c, h->Ephi, h->Exx, h->Eyy,
+            site(h, EFSI_SITE_COMBINE, 8.0 * N * (4.0 + 4.0 * nE + 4.0 + (rc ? 2.0 + 2.0 * st : 0.0)), [&] {
+                launch_combine_scalars(P, st, dtp, h->phi, h->sxn, h->syn, h->sxyn, h->c, h->Ephi, h->Exx, h->Eyy,
                                        h->Exy, rc ? h->Ec : nullptr, (rc && h->diff) ? h->Ic : nullptr, h->phis,
                                        h->sxs, h->sys, h->sxys, rc ? (h->diff ? h->rhs_c : h->cs) : nullptr, s);
             });
@@ -630,18 +717,22 @@ void enqueue_step(efsi_handle* h, double t, double dt) {
             if (rc) {
                 cstage = h->cs;
                 if (h->diff) {
-                    double alpha = dt * c_AI_diag[st];
-                    diff_init(P, alpha, P.nu.linear_reltol, std::max(1, P.nu.linear_maxiter), h->c, h->rhs_c, h->phis,
-                              h->ds, &d->cg_diff, h->slot[0], s);
-                    h->launches += 1;
-                    int it = run_cg(
-                        h, &d->cg_diff, std::max(1, P.nu.linear_maxiter), h->pred_diff,
-                        [&](int k) { diff_iter(P, alpha, h->phis, h->ds, k, &d->cg_diff, h->slot[1], h->slot[2], s); },
-                        3, 1);
-                    h->stats.resource_iterations[st] = std::abs(it);
+                    DtCoef alpha{dtp, c_AI_diag[st]};
+                    const int maxit = std::max(1, P.nu.linear_maxiter);
+                    solve(
+                        h, KIND_DIFF, st, &d->cg_diff, maxit, 6, 2,
+                        [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
+                            diff_init(P, alpha, P.nu.linear_reltol, maxit, h->c, h->rhs_c, h->phis, h->ds,
+                                      &d->cg_diff, h->slot[0], io, ch, ss);
+                            h->launches += 1;
+                        },
+                        [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
+                            for (int k = 0; k < 2; ++k)
+                                diff_iter(P, alpha, h->phis, h->ds, &d->cg_diff, h->slot[1], h->slot[2], io, ch, ss);
+                        });
                 }
             }
-            f = stage_fields(h->Us, h->Vs, h->phis, cstage, h->sxs, h->sys, h->sxys, Gp);
+            f = StageFields{h->Us, h->Vs, h->phis, cstage, h->sxs, h->sys, h->sxys, Gp};
         }
         if (h->growth) {
             launch_growth(P, f.phi, f.c, h->G, &d->max_trace, h->slot[0], s);
@@ -651,57 +742,170 @@ void enqueue_step(efsi_handle* h, double t, double dt) {
             launch_stage1_check(P, h->U, h->V, Gp, &d->max_constraint, h->slot[0], &d->st, s);
             h->launches += 1;
         } else {
-            site(h, EFSI_SITE_VEL_RHS, 8.0 * (double)h->nc * (4.0 + 4.0 * st), [&] {
-                launch_velocity_rhs(P, st, dt, h->U, h->V, h->Eu, h->Ev, h->Iu, h->Iv, h->phis, h->rhs_u, h->rhs_v,
-                                    s);
+            site(h, EFSI_SITE_VEL_RHS, 8.0 * N * (4.0 + 4.0 * st), [&] {
+                launch_velocity_rhs(P, st, dtp, h->U, h->V, h->Eu, h->Ev, h->Iu, h->Iv, h->phis, h->rhs_u,
+                                    h->rhs_v, s);
             });
             h->launches += 1;
             if (h->visc) {
-                double alpha = dt * c_AI_diag[st];
-                visc_init(P, alpha, P.nu.linear_reltol, std::max(1, P.nu.linear_maxiter), h->U, h->V, h->rhs_u,
-                          h->rhs_v, h->phis, h->vs, &d->cg_visc, h->slot[0], s);
-                h->launches += 2;
-                int it = run_cg(
-                    h, &d->cg_visc, std::max(1, P.nu.linear_maxiter), h->pred_visc,
-                    [&](int k) {
-                        const double N = (double)h->nc;
-                        site(h, EFSI_SITE_VISC_MATVEC, 8.0 * N * (k == 0 ? 10.0 : 12.0), [&] {
-                            visc_matvec(P, alpha, h->phis, h->vs, k, &d->cg_visc, h->slot[1], s);
-                        });
-                        site(h, EFSI_SITE_VISC_UPDATE, 8.0 * N * 14.0, [&] {
-                            visc_update(P, alpha, h->phis, h->vs, k, &d->cg_visc, h->slot[2], s);
-                        });
+                DtCoef alpha{dtp, c_AI_diag[st]};
+                const int maxit = std::max(1, P.nu.linear_maxiter);
+                solve(
+                    h, KIND_VISC, st, &d->cg_visc, maxit, 6, 2,
+                    [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
+                        visc_init(P, alpha, P.nu.linear_reltol, maxit, h->U, h->V, h->rhs_u, h->rhs_v, h->phis,
+                                  h->vs, &d->cg_visc, h->slot[0], io, ch, ss);
+                        h->launches += 2;
                     },
-                    3, 0);
-                h->stats.velocity_iterations[st] = std::abs(it);
+                    [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
+                        for (int k = 0; k < 2; ++k) {
+                            site(h, EFSI_SITE_VISC_MATVEC, 8.0 * N * 12.0, [&] {
+                                visc_matvec(P, alpha, h->phis, h->vs, &d->cg_visc, h->slot[1], ss);
+                            });
+                            site(h, EFSI_SITE_VISC_UPDATE, 8.0 * N * 14.0, [&] {
+                                visc_update(P, h->vs, &d->cg_visc, h->slot[2], io, ch, ss);
+                            });
+                        }
+                    });
             } else {
                 visc_enforce_dirichlet(P, h->rhs_u, h->rhs_v, h->vs.x_u, h->vs.x_v, s);
                 h->launches += 1;
             }
             projection(h, true, h->vs.x_u, h->vs.x_v, Gp, h->Us, h->Vs, st);
         }
-        if (st < 3) tendencies(h, st, t + c_CS[st] * dt, f);
+        if (st < 3) tendencies(h, st, f);
     }
     site(h, EFSI_SITE_FINALIZE, 16.0 * (double)(h->nu + h->nv + 5 * h->nc), [&] {
         launch_finalize(P, h->Us, h->Vs, h->phis, h->resource ? h->cs : h->c, h->sxs, h->sys, h->sxys, h->U, h->V,
                         h->phi, h->c, h->sxx, h->syy, h->sxy, d->report, &d->nonspd, h->slot[0], h->slot[1], &d->st,
                         s);
     });
-    h->launches += 1;
-    h->stats.kernel_launches = h->launches;
+    k_end_step<<<1, 1, 0, s>>>(d, h->hist_dev);
+    h->launches += 2;
 }
 
-void fill_report(efsi_handle* h, efsi_step_report* r) {
-    if (!r) return;
-    const DevBlock& b = *h->host;
-    r->maximum_projection_constraint_linf = b.max_constraint;
-    r->maximum_growth_trace_error = b.max_trace;
-    r->minimum_phi = b.report[0];
-    r->maximum_phi = b.report[1];
-    r->minimum_resource = b.report[2];
-    r->minimum_sigma_eigenvalue = b.report[3];
-    r->maximum_abs_sigma_determinant_error = b.report[4];
-    r->non_spd_cells = b.nonspd;
+// Capture the step once as a CUDA graph (CG loops become device-terminated WHILE
+// nodes).  If the driver refuses any part, the handle falls back to host-driven
+// stepping.
+void ensure_graph(efsi_handle* h) {
+    if (!h->use_graph || h->step_exec) return;
+    h->capturing = true;
+    h->loops.clear();
+    h->launches = 0;
+    bool ok = true;
+    try {
+        check_cuda(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "capture");
+        try {
+            enqueue_step(h);
+        } catch (...) {
+            cudaGraph_t junk = nullptr;
+            cudaStreamCaptureStatus cs2 = cudaStreamCaptureStatusNone;
+            if (cudaStreamIsCapturing(h->stream2, &cs2) == cudaSuccess && cs2 != cudaStreamCaptureStatusNone)
+                cudaStreamEndCapture(h->stream2, &junk);  // a body graph is owned by its node
+            junk = nullptr;
+            cudaStreamEndCapture(h->stream, &junk);
+            if (junk) cudaGraphDestroy(junk);
+            throw;
+        }
+        cudaGraph_t g = nullptr;
+        check_cuda(cudaStreamEndCapture(h->stream, &g), "capture");
+        h->step_graph = g;
+        check_cuda(cudaGraphInstantiate(&h->step_exec, g, 0), "graph instantiate");
+    } catch (const Err&) {
+        ok = false;
+    }
+    h->capturing = false;
+    h->fixed_launches = h->launches;
+    if (!ok) {
+        cudaGetLastError();
+        if (h->step_exec) { cudaGraphExecDestroy(h->step_exec); h->step_exec = nullptr; }
+        if (h->step_graph) { cudaGraphDestroy(h->step_graph); h->step_graph = nullptr; }
+        h->use_graph = false;
+    }
+}
+
+// Kernel launches of the last graph step, from its recorded iteration counts.
+long long graph_launches(const efsi_handle* h, const StepRec& r) {
+    long long n = h->fixed_launches;
+    for (const auto& l : h->loops)  // a body runs whole; its later iterations return at once
+        n += (long long)((r.iters[l.kind][l.stage] + l.iters_per_body - 1) / l.iters_per_body) * l.kernels_per_body;
+    return n;
+}
+
+void fill_report_rec(const StepRec& r, efsi_step_report* out) {
+    if (!out) return;
+    out->maximum_projection_constraint_linf = r.v[0];
+    out->maximum_growth_trace_error = r.v[1];
+    out->minimum_phi = r.v[2];
+    out->maximum_phi = r.v[3];
+    out->minimum_resource = r.v[4];
+    out->minimum_sigma_eigenvalue = r.v[5];
+    out->maximum_abs_sigma_determinant_error = r.v[6];
+    out->non_spd_cells = r.nonspd;
+}
+
+// n steps from (t0, dts): batches of up to kMaxBatch steps, each either graph
+// launches or host-driven enqueues, with one host synchronisation per batch.
+void run_steps(efsi_handle* h, double t0, const double* dts, int n, efsi_step_report* reports) {
+    for (int k = 0; k < n; ++k)
+        if (!std::isfinite(dts[k]) || !(dts[k] > 0)) throw Err{EFSI_ARG, "dt must be finite and strictly positive."};
+    if (!std::isfinite(t0)) throw Err{EFSI_ARG, "t must be finite."};
+    if (h->timed_site != EFSI_SITE_NONE) {
+        // per-launch events cannot live inside graph loops: time sites host-driven
+    } else {
+        ensure_graph(h);
+    }
+    const bool graph = h->step_exec && h->timed_site == EFSI_SITE_NONE;
+    long long launches = 0;
+    int32_t its[3][4] = {};
+    k_reset_call<<<1, 1, 0, h->stream>>>(h->dev);
+    double t = t0;
+    for (int base = 0; base < n; base += kMaxBatch) {
+        const int m = std::min(kMaxBatch, n - base);
+        check_cuda(cudaStreamSynchronize(h->stream), "batch");  // the pinned time buffer is free again
+        for (int k = 0; k < m; ++k) {
+            h->times_pinned[2 * k] = t;
+            h->times_pinned[2 * k + 1] = dts[base + k];
+            t += dts[base + k];
+        }
+        check_cuda(cudaMemcpyAsync(h->times_dev, h->times_pinned, 2 * m * sizeof(double), cudaMemcpyHostToDevice,
+                                   h->stream), "times");
+        if (base > 0) {  // restart the batch counter, keep the sticky status
+            check_cuda(cudaMemsetAsync(&h->dev->counter, 0, sizeof(int), h->stream), "counter");
+        }
+        for (int k = 0; k < m; ++k) {
+            if (graph) {
+                check_cuda(cudaGraphLaunch(h->step_exec, h->stream), "graph launch");
+            } else {
+                h->launches = 0;
+                enqueue_step(h);
+                launches += h->launches;
+            }
+        }
+        check_cuda(cudaMemcpyAsync(h->hist_pinned, h->hist_dev, m * sizeof(StepRec), cudaMemcpyDeviceToHost, h->stream),
+                   "history");
+        fetch_dev(h);
+        for (int k = 0; k < m; ++k) {
+            const StepRec& r = h->hist_pinned[k];
+            if (graph) launches += graph_launches(h, r);
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 4; ++b) its[a][b] += r.iters[a][b];
+        }
+        if (h->host->st.code != 0) {
+            Err e = decode(h->host->st);
+            int failed = base + std::max(h->host->first_fail, 0);
+            if (n > 1) e.msg = "step " + std::to_string(failed + 1) + " of " + std::to_string(n) + ": " + e.msg;
+            throw e;
+        }
+        if (reports)
+            for (int k = 0; k < m; ++k) fill_report_rec(h->hist_pinned[k], &reports[base + k]);
+    }
+    h->stats.kernel_launches = launches;
+    for (int b = 0; b < 4; ++b) {
+        h->stats.projection_iterations[b] = its[KIND_PROJ][b];
+        h->stats.velocity_iterations[b] = its[KIND_VISC][b];
+        h->stats.resource_iterations[b] = its[KIND_DIFF][b];
+    }
 }
 
 template <class F>
@@ -838,6 +1042,12 @@ int efsi_create(const efsi_config* cfg, efsi_handle** out) {
         check_cuda(cudaMallocHost(&h->host, sizeof(DevBlock)), "pinned");
         check_cuda(cudaMallocHost(&h->done_pinned, 4 * sizeof(int)), "pinned");
         std::memset(h->host, 0, sizeof(DevBlock));
+        h->times_dev = h->dalloc<double>(2 * (size_t)kMaxBatch);
+        h->hist_dev = h->dalloc<StepRec>(kMaxBatch);
+        check_cuda(cudaMallocHost(&h->times_pinned, 2 * (size_t)kMaxBatch * sizeof(double)), "pinned");
+        check_cuda(cudaMallocHost(&h->hist_pinned, (size_t)kMaxBatch * sizeof(StepRec)), "pinned");
+        check_cuda(cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking), "stream");
+        if (const char* e = std::getenv("EFSI_STEP_GRAPH")) h->use_graph = std::strcmp(e, "0") != 0;
         // default state: rest, sigma = I (the workspace's initial values)
         std::vector<double> ones(N, 1.0);
         check_cuda(cudaMemcpy(h->sxx, ones.data(), N * sizeof(double), cudaMemcpyHostToDevice), "init");
@@ -899,13 +1109,15 @@ int efsi_make_velocity_compatible(efsi_handle* h, efsi_projection_result* r) {
         DevBlock* d = h->dev;
         reset_call_stats(h);
         call_begin(h);
-        k_reset_block<<<1, 1, 0, h->stream>>>(d);
+        k_reset_call<<<1, 1, 0, h->stream>>>(d);
         launch_prepare_step(P, h->U, h->V, h->phi, h->c, h->sxx, h->syy, h->sxy, h->sxn, h->syn, h->sxyn, &d->st,
                             h->stream);
+        h->launches += 2;
         const double* Gp = nullptr;
         if (h->growth) {
             launch_growth(P, h->phi, h->c, h->G, &d->max_trace, h->slot[0], h->stream);
             Gp = h->G;
+            h->launches += 1;
         }
         // project! of state.U/V in place: the predictor is copied to Up/Vp first.
         projection(h, false, h->U, h->V, Gp, h->U, h->V, 0);
@@ -918,6 +1130,7 @@ int efsi_make_velocity_compatible(efsi_handle* h, efsi_projection_result* r) {
             r->constraint_l2 = h->host->ps.v[9];
             r->compatibility_defect = h->pj.nullspace ? h->host->ps.v[0] : 0.0;
         }
+        h->stats.projection_iterations[0] = h->host->iters[KIND_PROJ][0];
         h->stats.kernel_launches = h->launches;
     });
 }
@@ -929,12 +1142,10 @@ int efsi_integrate_step(efsi_handle* h, double t, double dt, efsi_step_report* r
         if (!(dt > 0)) throw Err{EFSI_ARG, "dt must be strictly positive."};
         if (h->step_block.code != EFSI_OK) throw h->step_block;
         reset_call_stats(h);
+        ensure_graph(h);
         call_begin(h);
-        enqueue_step(h, t, dt);
+        run_steps(h, t, &dt, 1, report);
         call_end(h);
-        fetch_dev(h);
-        raise_if_failed(h);
-        fill_report(h, report);
     });
 }
 
@@ -947,24 +1158,19 @@ int efsi_integrate_step_host(efsi_handle* h, double* U, double* V, double* phi, 
         if (!(dt > 0)) throw Err{EFSI_ARG, "dt must be strictly positive."};
         if (h->step_block.code != EFSI_OK) throw h->step_block;
         reset_call_stats(h);
+        ensure_graph(h);
         call_begin(h);
         h2d(h, h->U, U, h->nu); h2d(h, h->V, V, h->nv); h2d(h, h->phi, phi, h->nc);
         if (c) h2d(h, h->c, c, h->nc);
         else check_cuda(cudaMemsetAsync(h->c, 0, h->nc * sizeof(double), h->stream), "upload");
         h2d(h, h->sxx, sxx, h->nc); h2d(h, h->syy, syy, h->nc); h2d(h, h->sxy, sxy, h->nc);
         if (q) h2d(h, h->q, q, h->nc);
-        enqueue_step(h, t, dt);
-        fetch_dev(h);
-        if (h->host->st.code != 0) {
-            call_end(h);
-            throw decode(h->host->st);
-        }
+        run_steps(h, t, &dt, 1, report);  // throws before any download when the step fails
         d2h(h, U, h->U, h->nu); d2h(h, V, h->V, h->nv); d2h(h, phi, h->phi, h->nc);
         if (c) d2h(h, c, h->c, h->nc);
         d2h(h, sxx, h->sxx, h->nc); d2h(h, syy, h->syy, h->nc); d2h(h, sxy, h->sxy, h->nc);
         if (q) d2h(h, q, h->q, h->nc);
         call_end(h);
-        fill_report(h, report);
     });
 }
 
@@ -972,44 +1178,19 @@ int efsi_step_n(efsi_handle* h, double t0, const double* dts, int32_t n, efsi_st
     return guarded(h, [&] {
         if (n < 0 || (n > 0 && !dts)) throw Err{EFSI_ARG, "dts must hold n step sizes"};
         if (h->step_block.code != EFSI_OK) throw h->step_block;
-        for (int k = 0; k < n; ++k)
-            if (!std::isfinite(dts[k]) || !(dts[k] > 0)) throw Err{EFSI_ARG, "dt must be finite and strictly positive."};
-        double t = t0;
-        long long launches = 0;
-        int32_t it_proj[4] = {0, 0, 0, 0}, it_visc[4] = {0, 0, 0, 0};
         reset_call_stats(h);
-        call_begin(h);  // one event pair spans all n steps, host round trips included
-        for (int k = 0; k < n; ++k) {
-            h->launches = 0;
-            enqueue_step(h, t, dts[k]);
-            launches += h->launches;
-            for (int q = 0; q < 4; ++q) {
-                it_proj[q] += h->stats.projection_iterations[q];
-                it_visc[q] += h->stats.velocity_iterations[q];
-            }
-            fetch_dev(h);
-            if (h->host->st.code != 0) {
-                call_end(h);
-                Err e = decode(h->host->st);
-                e.msg = "step " + std::to_string(k + 1) + " of " + std::to_string(n) + ": " + e.msg;
-                throw e;
-            }
-            if (reports) fill_report(h, &reports[k]);
-            t += dts[k];
-        }
+        ensure_graph(h);
+        call_begin(h);  // one event pair spans all n steps
+        if (n > 0) run_steps(h, t0, dts, n, reports);
         call_end(h);
-        h->stats.kernel_launches = launches;
-        for (int q = 0; q < 4; ++q) {  // summed over the n steps
-            h->stats.projection_iterations[q] = it_proj[q];
-            h->stats.velocity_iterations[q] = it_visc[q];
-        }
     });
 }
 
 int efsi_project(efsi_handle* h, double* U, double* V, const double* target, efsi_projection_result* r) {
     return guarded(h, [&] {
         DevBlock* d = h->dev;
-        k_reset_block<<<1, 1, 0, h->stream>>>(d);
+        reset_call_stats(h);
+        k_reset_call<<<1, 1, 0, h->stream>>>(d);
         h2d(h, h->Us, U, h->nu);
         h2d(h, h->Vs, V, h->nv);
         const double* Gp = nullptr;
@@ -1026,6 +1207,8 @@ int efsi_project(efsi_handle* h, double* U, double* V, const double* target, efs
             r->constraint_l2 = h->host->ps.v[9];
             r->compatibility_defect = h->pj.nullspace ? h->host->ps.v[0] : 0.0;
         }
+        h->stats.projection_iterations[0] = h->host->iters[KIND_PROJ][0];
+        h->stats.kernel_launches = h->launches;
     });
 }
 
@@ -1033,11 +1216,11 @@ int efsi_phase_field_rhs(efsi_handle* h, const double* U, const double* V, const
                          double* rhs) {
     return guarded(h, [&] {
         DevBlock* d = h->dev;
-        k_reset_block<<<1, 1, 0, h->stream>>>(d);
+        k_reset_call<<<1, 1, 0, h->stream>>>(d);
         h2d(h, h->Us, U, h->nu); h2d(h, h->Vs, V, h->nv); h2d(h, h->phis, phi, h->nc);
         const double* Gp = nullptr;
         if (G) { h2d(h, h->G, G, h->nc); Gp = h->G; }
-        StageFields f = stage_fields(h->Us, h->Vs, h->phis, h->c, h->sxs, h->sys, h->sxys, Gp);
+        StageFields f{h->Us, h->Vs, h->phis, h->c, h->sxs, h->sys, h->sxys, Gp};
         if (h->P.md.phase_field_method == EFSI_PF_ACDI && h->P.md.pf_option)
             launch_umax(h->P, f.U, f.V, &d->gamma_dyn, h->slot[0], h->stream);
         launch_phase_rhs(h->P, f, &d->gamma_dyn, h->Ephi[0], &d->st, h->stream);
@@ -1053,12 +1236,12 @@ int efsi_structure_tensor_rhs(efsi_handle* h, const double* sxx, const double* s
                               double* ryy, double* rxy) {
     return guarded(h, [&] {
         DevBlock* d = h->dev;
-        k_reset_block<<<1, 1, 0, h->stream>>>(d);
+        k_reset_call<<<1, 1, 0, h->stream>>>(d);
         h2d(h, h->Us, U, h->nu); h2d(h, h->Vs, V, h->nv); h2d(h, h->phis, phi, h->nc);
         h2d(h, h->sxs, sxx, h->nc); h2d(h, h->sys, syy, h->nc); h2d(h, h->sxys, sxy, h->nc);
         const double* Gp = nullptr;
         if (G) { h2d(h, h->G, G, h->nc); Gp = h->G; }
-        StageFields f = stage_fields(h->Us, h->Vs, h->phis, h->c, h->sxs, h->sys, h->sxys, Gp);
+        StageFields f{h->Us, h->Vs, h->phis, h->c, h->sxs, h->sys, h->sxys, Gp};
         launch_structure_rhs(h->P, f, h->Exx[0], h->Eyy[0], h->Exy[0], &d->st, h->stream);
         fetch_dev(h);
         raise_if_failed(h);
@@ -1072,12 +1255,12 @@ int efsi_momentum_explicit_rhs(efsi_handle* h, double t, const double* U, const 
                                double* Fy) {
     return guarded(h, [&] {
         DevBlock* d = h->dev;
-        k_reset_block<<<1, 1, 0, h->stream>>>(d);
+        k_reset_call<<<1, 1, 0, h->stream>>>(d);
         h2d(h, h->Us, U, h->nu); h2d(h, h->Vs, V, h->nv); h2d(h, h->phis, phi, h->nc);
         h2d(h, h->sxs, sxx, h->nc); h2d(h, h->sys, syy, h->nc); h2d(h, h->sxys, sxy, h->nc);
         const double* Gp = nullptr;
         if (G) { h2d(h, h->G, G, h->nc); Gp = h->G; }
-        StageFields f = stage_fields(h->Us, h->Vs, h->phis, h->c, h->sxs, h->sys, h->sxys, Gp);
+        StageFields f{h->Us, h->Vs, h->phis, h->c, h->sxs, h->sys, h->sxys, Gp};
         const double* kappa = nullptr;
         if (h->P.md.capillarity == EFSI_CAP_DIFFUSE_AREA) {
             launch_capillary_curvature(h->P, f.phi, h->cap_a, h->cap_b, h->kappa, h->stream);

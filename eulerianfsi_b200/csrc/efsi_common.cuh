@@ -88,6 +88,19 @@ __device__ __forceinline__ void raise_err(DevStatus* st, int code, int where, in
     }
 }
 
+// Time-step dependent coefficient read from device memory (dt * coef), so that a
+// captured CUDA graph of the step is valid for every dt.
+struct DtCoef {
+    const double* dt;
+    double coef;
+    __device__ __forceinline__ double value() const { return *dt * coef; }
+};
+
+// Loop control of a CUDA-graph WHILE node: 0 when the kernel runs outside a graph.
+__device__ __forceinline__ void set_loop(cudaGraphConditionalHandle h, bool keep_going) {
+    if (h) cudaGraphSetConditional(h, keep_going ? 1u : 0u);
+}
+
 // ---- indexing ------------------------------------------------------------------------------
 __device__ __forceinline__ int wrapi(int k, int n) { return k < 0 ? k + n : (k >= n ? k - n : k); }
 __device__ __forceinline__ size_t cidx(int i, int j, int Nx) { return (size_t)i + (size_t)j * Nx; }

@@ -14,12 +14,12 @@ struct StageFields {
 void launch_prepare_step(const Params& P, const double* U, const double* V, const double* phi,
                          const double* c, const double* sxx, const double* syy, const double* sxy,
                          double* sxn, double* syn, double* sxyn, DevStatus* st, cudaStream_t s);
-void launch_combine_scalars(const Params& P, int stage, double dt, const double* phin,
+void launch_combine_scalars(const Params& P, int stage, const double* dt, const double* phin,
                             const double* sxn, const double* syn, const double* sxyn, const double* cn,
                             double* const* Ephi, double* const* Exx, double* const* Eyy,
                             double* const* Exy, double* const* Ec, double* const* Ic, double* phis,
                             double* sxs, double* sys, double* sxys, double* cs_or_rhs, cudaStream_t s);
-void launch_velocity_rhs(const Params& P, int stage, double dt, const double* Un, const double* Vn,
+void launch_velocity_rhs(const Params& P, int stage, const double* dt, const double* Un, const double* Vn,
                          double* const* Eu, double* const* Ev, double* const* Iu, double* const* Iv,
                          const double* phis, double* rhs_u, double* rhs_v, cudaStream_t s);
 void launch_growth(const Params& P, const double* phi, const double* c, double* G, double* trace_max,

@@ -69,7 +69,7 @@ struct HistPtrs {
     const double* p[3];
 };
 
-__global__ void k_combine_scalars(Params P, int s, double dt, const double* __restrict__ phin,
+__global__ void k_combine_scalars(Params P, int s, const double* __restrict__ dtp, const double* __restrict__ phin,
                                   const double* __restrict__ sxn, const double* __restrict__ syn,
                                   const double* __restrict__ sxyn, const double* __restrict__ cn, HistPtrs Ephi,
                                   HistPtrs Exx, HistPtrs Eyy, HistPtrs Exy, HistPtrs Ec, HistPtrs Ic, double* phis,
@@ -77,6 +77,7 @@ __global__ void k_combine_scalars(Params P, int s, double dt, const double* __re
     const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
     const int Nx = P.g.Nx;
     if (i >= Nx || j >= P.g.Ny) return;
+    const double dt = *dtp;
     size_t k = cidx(i, j, Nx);
     double p = phin[k], a = sxn[k], d = syn[k], b = sxyn[k], r = cn[k];
     for (int q = 0; q < s; ++q) {
@@ -149,7 +150,7 @@ __global__ void k_combine_scalars(Params P, int s, double dt, const double* __re
     }
 }
 
-void launch_combine_scalars(const Params& P, int stage, double dt, const double* phin, const double* sxn,
+void launch_combine_scalars(const Params& P, int stage, const double* dt, const double* phin, const double* sxn,
                             const double* syn, const double* sxyn, const double* cn, double* const* Ephi,
                             double* const* Exx, double* const* Eyy, double* const* Exy, double* const* Ec,
                             double* const* Ic, double* phis, double* sxs, double* sys, double* sxys,
@@ -185,12 +186,13 @@ __device__ __forceinline__ void visc_boundary(const Params& P, const MuField& mu
     }
 }
 
-__global__ void k_velocity_rhs(Params P, int s, double dt, const double* __restrict__ Un,
+__global__ void k_velocity_rhs(Params P, int s, const double* __restrict__ dtp, const double* __restrict__ Un,
                                const double* __restrict__ Vn, HistPtrs Eu, HistPtrs Ev, HistPtrs Iu, HistPtrs Iv,
                                const double* __restrict__ phis, double* rhs_u, double* rhs_v) {
     const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
     const int Nx = P.g.Nx, Ny = P.g.Ny;
     if (i >= Nx || j >= Ny) return;
+    const double dt = *dtp;
     size_t k = cidx(i, j, Nx);
     double ru = Un[uidx(i, j, Nx)], rv = Vn[vidx(i, j, Nx)];
     for (int q = 0; q < s; ++q) {  // TimeIntegrationIMEX.jl:777-784
@@ -212,7 +214,7 @@ __global__ void k_velocity_rhs(Params P, int s, double dt, const double* __restr
     rhs_v[k] = rv;
 }
 
-void launch_velocity_rhs(const Params& P, int stage, double dt, const double* Un, const double* Vn,
+void launch_velocity_rhs(const Params& P, int stage, const double* dt, const double* Un, const double* Vn,
                          double* const* Eu, double* const* Ev, double* const* Iu, double* const* Iv,
                          const double* phis, double* rhs_u, double* rhs_v, cudaStream_t s) {
     HistPtrs a{}, b{}, c{}, d{};

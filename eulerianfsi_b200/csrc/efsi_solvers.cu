@@ -119,13 +119,15 @@ __global__ void k_visc_x0(Params P, const double* __restrict__ Un, const double*
     xv[k] = v_fixed(P, j) ? bval(P.bv.s[BOTTOM], i) : Vn[vidx(i, j, Nx)];
 }
 
-__global__ void k_visc_init(Params P, double alpha, double reltol, int maxiter, const double* __restrict__ xu,
+__global__ void k_visc_init(Params P, DtCoef ac, double reltol, int maxiter, const double* __restrict__ xu,
                             const double* __restrict__ xv, const double* __restrict__ rhs_u,
                             const double* __restrict__ rhs_v, const double* __restrict__ phi, double* ru, double* rv,
-                            double* dinv_u, double* dinv_v, CGScal* cg, RedSlot rs) {
+                            double* dinv_u, double* dinv_v, CGScal* cg, RedSlot rs, int* iters_out,
+                            cudaGraphConditionalHandle cond) {
     __shared__ double sh[64];
     const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
     const int Nx = P.g.Nx;
+    const double alpha = ac.value();
     double acc[2] = {0.0, 0.0};
     if (i < Nx && j < P.g.Ny) {
         MuField mu = make_mu(P, phi);
@@ -155,15 +157,18 @@ __global__ void k_visc_init(Params P, double alpha, double reltol, int maxiter, 
         cg->maxiter = maxiter;
         cg->beta = 0.0;
         cg->conv = tot[0] == 0.0 ? 1 : 0;
-        cg->done = cg->conv;
+        cg->done = (cg->conv || !isfinite(tot[0])) ? 1 : 0;  // a non-finite start ends at once
+        if (iters_out) *iters_out = 0;
+        set_loop(cond, !cg->done);
     }
 }
 
 // p = D^-1 r + beta*p (Jacobi-preconditioned search direction; zero on Dirichlet rows).
-__global__ void k_visc_pupdate(int n, int first, const double* __restrict__ ru, const double* __restrict__ rv,
+__global__ void k_visc_pupdate(int n, const double* __restrict__ ru, const double* __restrict__ rv,
                                const double* __restrict__ dinv_u, const double* __restrict__ dinv_v, double* pu,
                                double* pv, const CGScal* cg) {
     if (cg->done) return;
+    const int first = cg->iter == 0;
     const double beta = first ? 0.0 : cg->beta;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         double a = ru[k] * dinv_u[k], b = rv[k] * dinv_v[k];
@@ -173,10 +178,11 @@ __global__ void k_visc_pupdate(int n, int first, const double* __restrict__ ru, 
 }
 
 // Ap = (I - alpha*A) p on the free rows (0 on Dirichlet rows), partial p.Ap -> alpha_cg.
-__global__ void k_visc_matvec(Params P, double alpha, const double* __restrict__ phi, const double* __restrict__ pu,
+__global__ void k_visc_matvec(Params P, DtCoef ac, const double* __restrict__ phi, const double* __restrict__ pu,
                               const double* __restrict__ pv, double* Apu, double* Apv, CGScal* cg, RedSlot rs) {
     __shared__ double sh[32];
     if (cg->done) return;
+    const double alpha = ac.value();
     const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
     const int Nx = P.g.Nx, Ny = P.g.Ny;
     double acc[1] = {0.0};
@@ -203,7 +209,8 @@ __global__ void k_visc_matvec(Params P, double alpha, const double* __restrict__
 __global__ void k_visc_update(Params P, const double* __restrict__ dinv_u, const double* __restrict__ dinv_v,
                               double* xu, double* xv, double* ru, double* rv, const double* __restrict__ pu,
                               const double* __restrict__ pv, const double* __restrict__ Apu,
-                              const double* __restrict__ Apv, CGScal* cg, RedSlot rs) {
+                              const double* __restrict__ Apv, CGScal* cg, RedSlot rs, int* iters_out,
+                              cudaGraphConditionalHandle cond) {
     __shared__ double sh[64];
     if (cg->done) return;
     const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
@@ -227,36 +234,33 @@ __global__ void k_visc_update(Params P, const double* __restrict__ dinv_u, const
         cg->rz = tot[1];
         if (tot[0] <= cg->tol2) { cg->conv = 1; cg->done = 1; }
         else if (cg->iter >= cg->maxiter || !isfinite(tot[0])) cg->done = 1;
+        if (iters_out) *iters_out = cg->iter;
+        set_loop(cond, !cg->done);
     }
 }
 
-void visc_init(const Params& P, double alpha, double reltol, int maxiter, const double* Un, const double* Vn,
+void visc_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const double* Un, const double* Vn,
                const double* rhs_u, const double* rhs_v, const double* phi, const ViscSolve& w, CGScal* cg,
-               const RedSlot& rs, cudaStream_t s) {
+               const RedSlot& rs, int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s) {
     dim3 g = grid2(P.g.Nx, P.g.Ny), b(BX, BY);
     k_visc_x0<<<g, b, 0, s>>>(P, Un, Vn, w.x_u, w.x_v);
     k_visc_init<<<g, b, 0, s>>>(P, alpha, reltol, maxiter, w.x_u, w.x_v, rhs_u, rhs_v, phi, w.r_u, w.r_v, w.dinv_u,
-                                w.dinv_v, cg, rs);
+                                w.dinv_v, cg, rs, iters_out, cond);
 }
 
-void visc_matvec(const Params& P, double alpha, const double* phi, const ViscSolve& w, int it, CGScal* cg,
-                 const RedSlot& rs, cudaStream_t s) {
+void visc_matvec(const Params& P, DtCoef alpha, const double* phi, const ViscSolve& w, CGScal* cg, const RedSlot& rs,
+                 cudaStream_t s) {
     const int n = P.g.Nx * P.g.Ny;
-    k_visc_pupdate<<<std::min((n + 255) / 256, 148 * 8), 256, 0, s>>>(n, it == 0, w.r_u, w.r_v, w.dinv_u, w.dinv_v,
-                                                                     w.p_u[0], w.p_v[0], cg);
+    k_visc_pupdate<<<std::min((n + 255) / 256, 148 * 8), 256, 0, s>>>(n, w.r_u, w.r_v, w.dinv_u, w.dinv_v, w.p_u[0],
+                                                                     w.p_v[0], cg);
     k_visc_matvec<<<grid2(P.g.Nx, P.g.Ny), dim3(BX, BY), 0, s>>>(P, alpha, phi, w.p_u[0], w.p_v[0], w.Ap_u, w.Ap_v,
                                                               cg, rs);
 }
-void visc_update(const Params& P, double alpha, const double* phi, const ViscSolve& w, int it, CGScal* cg,
-                 const RedSlot& rs, cudaStream_t s) {
-    (void)alpha; (void)phi; (void)it;
+void visc_update(const Params& P, const ViscSolve& w, CGScal* cg, const RedSlot& rs, int* iters_out,
+                 cudaGraphConditionalHandle cond, cudaStream_t s) {
     k_visc_update<<<grid2(P.g.Nx, P.g.Ny), dim3(BX, BY), 0, s>>>(P, w.dinv_u, w.dinv_v, w.x_u, w.x_v, w.r_u, w.r_v,
-                                                              w.p_u[0], w.p_v[0], w.Ap_u, w.Ap_v, cg, rs);
-}
-void visc_iter(const Params& P, double alpha, const double* phi, const ViscSolve& w, int it, CGScal* cg,
-               const RedSlot& rs1, const RedSlot& rs2, cudaStream_t s) {
-    visc_matvec(P, alpha, phi, w, it, cg, rs1, s);
-    visc_update(P, alpha, phi, w, it, cg, rs2, s);
+                                                              w.p_u[0], w.p_v[0], w.Ap_u, w.Ap_v, cg, rs, iters_out,
+                                                              cond);
 }
 
 // NoViscosity: predictor = rhs with the Dirichlet rows enforced (:786-788).
@@ -333,12 +337,13 @@ __device__ void diff_L(const Params& P, const double* phi, const F& f, int i, in
     diag = -(dx[0] + dx[1]) * ihx - (dy[0] + dy[1]) * ihy;
 }
 
-__global__ void k_diff_init(Params P, double alpha, double reltol, int maxiter, const double* __restrict__ c0,
+__global__ void k_diff_init(Params P, DtCoef ac, double reltol, int maxiter, const double* __restrict__ c0,
                             const double* __restrict__ rhs, const double* __restrict__ phi, double* x, double* r,
-                            double* dinv, CGScal* cg, RedSlot rs) {
+                            double* dinv, CGScal* cg, RedSlot rs, int* iters_out, cudaGraphConditionalHandle cond) {
     __shared__ double sh[64];
     const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
     const int Nx = P.g.Nx;
+    const double alpha = ac.value();
     double acc[2] = {0.0, 0.0};
     if (i < Nx && j < P.g.Ny) {
         auto f = [&](int a, int b) { return c0[cidx(a, b, Nx)]; };
@@ -359,13 +364,16 @@ __global__ void k_diff_init(Params P, double alpha, double reltol, int maxiter, 
         cg->tol2 = reltol * reltol * tot[0];
         cg->iter = 0; cg->maxiter = maxiter; cg->beta = 0.0;
         cg->conv = tot[0] == 0.0 ? 1 : 0;
-        cg->done = cg->conv;
+        cg->done = (cg->conv || !isfinite(tot[0])) ? 1 : 0;  // a non-finite start ends at once
+        if (iters_out) *iters_out = 0;
+        set_loop(cond, !cg->done);
     }
 }
 
-__global__ void k_diff_pupdate(int n, int first, const double* __restrict__ r, const double* __restrict__ dinv,
-                               double* p, const CGScal* cg) {
+__global__ void k_diff_pupdate(int n, const double* __restrict__ r, const double* __restrict__ dinv, double* p,
+                               const CGScal* cg) {
     if (cg->done) return;
+    const int first = cg->iter == 0;
     const double beta = first ? 0.0 : cg->beta;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         double z = r[k] * dinv[k];
@@ -373,10 +381,11 @@ __global__ void k_diff_pupdate(int n, int first, const double* __restrict__ r, c
     }
 }
 
-__global__ void k_diff_matvec(Params P, double alpha, const double* __restrict__ phi, const double* __restrict__ p,
+__global__ void k_diff_matvec(Params P, DtCoef ac, const double* __restrict__ phi, const double* __restrict__ p,
                               double* Ap, CGScal* cg, RedSlot rs) {
     __shared__ double sh[32];
     if (cg->done) return;
+    const double alpha = ac.value();
     const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
     const int Nx = P.g.Nx;
     double acc[1] = {0.0};
@@ -397,7 +406,8 @@ __global__ void k_diff_matvec(Params P, double alpha, const double* __restrict__
 }
 
 __global__ void k_diff_update(Params P, const double* __restrict__ dinv, double* x, double* r,
-                              const double* __restrict__ p, const double* __restrict__ Ap, CGScal* cg, RedSlot rs) {
+                              const double* __restrict__ p, const double* __restrict__ Ap, CGScal* cg, RedSlot rs,
+                              int* iters_out, cudaGraphConditionalHandle cond) {
     __shared__ double sh[64];
     if (cg->done) return;
     const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
@@ -420,21 +430,24 @@ __global__ void k_diff_update(Params P, const double* __restrict__ dinv, double*
         cg->rz = tot[1];
         if (tot[0] <= cg->tol2) { cg->conv = 1; cg->done = 1; }
         else if (cg->iter >= cg->maxiter || !isfinite(tot[0])) cg->done = 1;
+        if (iters_out) *iters_out = cg->iter;
+        set_loop(cond, !cg->done);
     }
 }
 
-void diff_init(const Params& P, double alpha, double reltol, int maxiter, const double* c0, const double* rhs,
-               const double* phi, const ScalarSolve& w, CGScal* cg, const RedSlot& rs, cudaStream_t s) {
+void diff_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const double* c0, const double* rhs,
+               const double* phi, const ScalarSolve& w, CGScal* cg, const RedSlot& rs, int* iters_out,
+               cudaGraphConditionalHandle cond, cudaStream_t s) {
     k_diff_init<<<grid2(P.g.Nx, P.g.Ny), dim3(BX, BY), 0, s>>>(P, alpha, reltol, maxiter, c0, rhs, phi, w.x, w.r,
-                                                              w.dinv, cg, rs);
+                                                              w.dinv, cg, rs, iters_out, cond);
 }
-void diff_iter(const Params& P, double alpha, const double* phi, const ScalarSolve& w, int it, CGScal* cg,
-               const RedSlot& rs1, const RedSlot& rs2, cudaStream_t s) {
+void diff_iter(const Params& P, DtCoef alpha, const double* phi, const ScalarSolve& w, CGScal* cg, const RedSlot& rs1,
+               const RedSlot& rs2, int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s) {
     dim3 g = grid2(P.g.Nx, P.g.Ny), b(BX, BY);
     const int n = P.g.Nx * P.g.Ny;
-    k_diff_pupdate<<<std::min((n + 255) / 256, 148 * 8), 256, 0, s>>>(n, it == 0, w.r, w.dinv, w.p[0], cg);
+    k_diff_pupdate<<<std::min((n + 255) / 256, 148 * 8), 256, 0, s>>>(n, w.r, w.dinv, w.p[0], cg);
     k_diff_matvec<<<g, b, 0, s>>>(P, alpha, phi, w.p[0], w.Ap, cg, rs1);
-    k_diff_update<<<g, b, 0, s>>>(P, w.dinv, w.x, w.r, w.p[0], w.Ap, cg, rs2);
+    k_diff_update<<<g, b, 0, s>>>(P, w.dinv, w.x, w.r, w.p[0], w.Ap, cg, rs2, iters_out, cond);
 }
 
 // =====================================================================================
@@ -733,7 +746,7 @@ void proj_rhs(const Params& P, const Projection& pj, bool compact_in, const doub
 // ---- CG on the fine level --------------------------------------------------------------------
 __global__ void k_pcg_init(MGLevel L, int px, int py, double reltol, int maxiter, const double* __restrict__ q0,
                            const double* __restrict__ b, double* x, double* r, const ProjScal* ps, CGScal* cg,
-                           RedSlot rs, const DevStatus* st) {
+                           RedSlot rs, const DevStatus* st, int* iters_out, cudaGraphConditionalHandle cond) {
     __shared__ double sh[32];
     const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
     const int nx = L.nx;
@@ -757,13 +770,16 @@ __global__ void k_pcg_init(MGLevel L, int px, int py, double reltol, int maxiter
         cg->conv = tot[0] == 0.0 ? 1 : 0;
         // a flagged step skips its solves (the state is not committed)
         cg->done = (cg->conv || st->code != 0) ? 1 : 0;
+        if (iters_out) *iters_out = 0;
+        set_loop(cond, !cg->done);
     }
 }
 
-__global__ void k_pcg_matvec(MGLevel L, int px, int py, int first, const double* __restrict__ z,
+__global__ void k_pcg_matvec(MGLevel L, int px, int py, const double* __restrict__ z,
                              const double* __restrict__ p_old, double* p, double* Ap, CGScal* cg, RedSlot rs) {
     __shared__ double sh[32];
     if (cg->done) return;
+    const int first = cg->iter == 0;
     const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
     const int nx = L.nx;
     const double beta = first ? 0.0 : cg->beta;
@@ -790,7 +806,8 @@ __global__ void k_pcg_matvec(MGLevel L, int px, int py, int first, const double*
 }
 
 __global__ void k_pcg_update(MGLevel L, double* x, double* r, const double* __restrict__ p,
-                             const double* __restrict__ Ap, CGScal* cg, RedSlot rs) {
+                             const double* __restrict__ Ap, CGScal* cg, RedSlot rs, int* iters_out,
+                             cudaGraphConditionalHandle cond) {
     __shared__ double sh[32];
     if (cg->done) return;
     const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
@@ -809,36 +826,35 @@ __global__ void k_pcg_update(MGLevel L, double* x, double* r, const double* __re
         cg->rr = tot[0];
         if (tot[0] <= cg->tol2) { cg->conv = 1; cg->done = 1; }
         else if (cg->iter >= cg->maxiter || !isfinite(tot[0])) cg->done = 1;
+        if (iters_out) *iters_out = cg->iter;
+        set_loop(cond, !cg->done);
     }
 }
 
 void proj_cg_init(const Params& P, const Projection& pj, double reltol, int maxiter, const double* q0, CGScal* cg,
-                  const ProjScal* ps, const RedSlot& rs, const RedSlot& rs2, const DevStatus* st, cudaStream_t s) {
+                  const ProjScal* ps, const RedSlot& rs, const RedSlot& rs2, const DevStatus* st, int* iters_out,
+                  cudaGraphConditionalHandle cond, cudaStream_t s) {
     const MGLevel& L = pj.lev[0];
     k_pcg_init<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, s>>>(L, P.g.px, P.g.py, reltol, maxiter, q0, pj.b, pj.x, pj.r,
-                                                          ps, cg, rs, st);
+                                                          ps, cg, rs, st, iters_out, cond);
     vcycle(pj, 0, pj.r, pj.z, cg, rs2, P.g.px, P.g.py, s);
 }
 
-void proj_matvec(const Params& P, const Projection& pj, int it, CGScal* cg, const RedSlot& rs, cudaStream_t s) {
+// One CG iteration; `parity` selects the search-direction buffers (p[parity] is written).
+void proj_matvec(const Params& P, const Projection& pj, int parity, CGScal* cg, const RedSlot& rs, cudaStream_t s) {
     const MGLevel& L = pj.lev[0];
-    const int cur = it & 1, old = cur ^ 1;
-    k_pcg_matvec<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, s>>>(L, P.g.px, P.g.py, it == 0, pj.z, pj.p[old], pj.p[cur],
-                                                            pj.Ap, cg, rs);
+    const int cur = parity & 1, old = cur ^ 1;
+    k_pcg_matvec<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, s>>>(L, P.g.px, P.g.py, pj.z, pj.p[old], pj.p[cur], pj.Ap, cg,
+                                                            rs);
 }
-void proj_update(const Params& P, const Projection& pj, int it, CGScal* cg, const RedSlot& rs, cudaStream_t s) {
+void proj_update(const Params& P, const Projection& pj, int parity, CGScal* cg, const RedSlot& rs, int* iters_out,
+                 cudaGraphConditionalHandle cond, cudaStream_t s) {
     const MGLevel& L = pj.lev[0];
-    const int cur = it & 1;
-    k_pcg_update<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, s>>>(L, pj.x, pj.r, pj.p[cur], pj.Ap, cg, rs);
+    const int cur = parity & 1;
+    k_pcg_update<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, s>>>(L, pj.x, pj.r, pj.p[cur], pj.Ap, cg, rs, iters_out, cond);
 }
 void proj_vcycle(const Params& P, const Projection& pj, CGScal* cg, const RedSlot& rs, cudaStream_t s) {
     vcycle(pj, 0, pj.r, pj.z, cg, rs, P.g.px, P.g.py, s);
-}
-void proj_cg_iter(const Params& P, const Projection& pj, int it, CGScal* cg, const RedSlot& rs1, const RedSlot& rs2,
-                  const RedSlot& rs3, cudaStream_t s) {
-    proj_matvec(P, pj, it, cg, rs1, s);
-    proj_update(P, pj, it, cg, rs2, s);
-    proj_vcycle(P, pj, cg, rs3, s);
 }
 
 // ---- correction and diagnostics (Projection.jl:253-306) ---------------------------------------

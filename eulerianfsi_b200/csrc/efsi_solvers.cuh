@@ -16,15 +16,13 @@ struct CGScal {
 struct ViscSolve {
     double *x_u, *x_v, *r_u, *r_v, *p_u[2], *p_v[2], *Ap_u, *Ap_v, *dinv_u, *dinv_v;
 };
-void visc_init(const Params& P, double alpha, double reltol, int maxiter, const double* Un, const double* Vn,
+void visc_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const double* Un, const double* Vn,
                const double* rhs_u, const double* rhs_v, const double* phi, const ViscSolve& w, CGScal* cg,
-               const RedSlot& rs, cudaStream_t s);
-void visc_iter(const Params& P, double alpha, const double* phi, const ViscSolve& w, int it, CGScal* cg,
-               const RedSlot& rs1, const RedSlot& rs2, cudaStream_t s);
-void visc_matvec(const Params& P, double alpha, const double* phi, const ViscSolve& w, int it, CGScal* cg,
-                 const RedSlot& rs, cudaStream_t s);
-void visc_update(const Params& P, double alpha, const double* phi, const ViscSolve& w, int it, CGScal* cg,
-                 const RedSlot& rs, cudaStream_t s);
+               const RedSlot& rs, int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s);
+void visc_matvec(const Params& P, DtCoef alpha, const double* phi, const ViscSolve& w, CGScal* cg, const RedSlot& rs,
+                 cudaStream_t s);
+void visc_update(const Params& P, const ViscSolve& w, CGScal* cg, const RedSlot& rs, int* iters_out,
+                 cudaGraphConditionalHandle cond, cudaStream_t s);
 void visc_enforce_dirichlet(const Params& P, const double* rhs_u, const double* rhs_v, double* x_u, double* x_v,
                             cudaStream_t s);
 
@@ -32,10 +30,11 @@ void visc_enforce_dirichlet(const Params& P, const double* rhs_u, const double* 
 struct ScalarSolve {
     double *x, *r, *p[2], *Ap, *dinv;
 };
-void diff_init(const Params& P, double alpha, double reltol, int maxiter, const double* c0, const double* rhs,
-               const double* phi, const ScalarSolve& w, CGScal* cg, const RedSlot& rs, cudaStream_t s);
-void diff_iter(const Params& P, double alpha, const double* phi, const ScalarSolve& w, int it, CGScal* cg,
-               const RedSlot& rs1, const RedSlot& rs2, cudaStream_t s);
+void diff_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const double* c0, const double* rhs,
+               const double* phi, const ScalarSolve& w, CGScal* cg, const RedSlot& rs, int* iters_out,
+               cudaGraphConditionalHandle cond, cudaStream_t s);
+void diff_iter(const Params& P, DtCoef alpha, const double* phi, const ScalarSolve& w, CGScal* cg, const RedSlot& rs1,
+               const RedSlot& rs2, int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s);
 
 // ---- projection ------------------------------------------------------------------------
 struct MGLevel {
@@ -63,15 +62,15 @@ struct ProjScal {
 void proj_rhs(const Params& P, const Projection& pj, bool compact_in, const double* u_in, const double* v_in,
               const double* G, ProjScal* ps, const RedSlot& rs, DevStatus* st, cudaStream_t s);
 void proj_cg_init(const Params& P, const Projection& pj, double reltol, int maxiter, const double* q0, CGScal* cg,
-                  const ProjScal* ps, const RedSlot& rs, const RedSlot& rs2, const DevStatus* st, cudaStream_t s);
-void proj_cg_iter(const Params& P, const Projection& pj, int it, CGScal* cg, const RedSlot& rs1,
-                  const RedSlot& rs2, const RedSlot& rs3, cudaStream_t s);
+                  const ProjScal* ps, const RedSlot& rs, const RedSlot& rs2, const DevStatus* st, int* iters_out,
+                  cudaGraphConditionalHandle cond, cudaStream_t s);
+void proj_matvec(const Params& P, const Projection& pj, int parity, CGScal* cg, const RedSlot& rs, cudaStream_t s);
+void proj_update(const Params& P, const Projection& pj, int parity, CGScal* cg, const RedSlot& rs, int* iters_out,
+                 cudaGraphConditionalHandle cond, cudaStream_t s);
+void proj_vcycle(const Params& P, const Projection& pj, CGScal* cg, const RedSlot& rs, cudaStream_t s);
 void proj_finish(const Params& P, const Projection& pj, const double* G, double* q_out, double* U_out,
                  double* V_out, ProjScal* ps, double* stage_linf, const RedSlot& rs1, const RedSlot& rs2,
                  DevStatus* st, cudaStream_t s);
-void proj_matvec(const Params& P, const Projection& pj, int it, CGScal* cg, const RedSlot& rs, cudaStream_t s);
-void proj_update(const Params& P, const Projection& pj, int it, CGScal* cg, const RedSlot& rs, cudaStream_t s);
-void proj_vcycle(const Params& P, const Projection& pj, CGScal* cg, const RedSlot& rs, cudaStream_t s);
 // Number of kernel launches of one projection CG iteration (statistics).
 int proj_kernels_per_iter(const Projection& pj);
 

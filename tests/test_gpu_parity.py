@@ -331,3 +331,69 @@ def test_phase_mass_conservation():
         ef.integrate_step(st, t, w.dt, ctx, work)
         t += w.dt
     assert abs(st.phi.sum() - m0) / m0 <= 1e-12
+
+
+def _graph_vs_host(w, steps):
+    from eulerianfsi_b200.imex import ConfigBlock, Handle
+    out = []
+    for timed in (-1, _abi.SITES.index("pcg_update")):  # a timed site forces host-driven stepping
+        h = Handle(_abi.load_library(), "efsi_", ConfigBlock(w.metrics, w.bcs, w.models, w.numerics), w.metrics)
+        h.call("set_timed_site", timed)
+        st = w.state.copy()
+        h.upload(st)
+        h.set_correction(fz(w.metrics.Nx, w.metrics.Ny))
+        h.call("make_velocity_compatible", C.byref(_abi.ProjectionResultC()))
+        dts = (C.c_double * steps)(*([w.dt] * steps))
+        reps = (_abi.StepReportC * steps)()
+        h.call("step_n", 0.0, dts, steps, reps)
+        s = h.stats()
+        h.download(st)
+        out.append((st, [ef.StepReport.from_c(r) for r in reps], s))
+    return out
+
+
+@pytest.mark.parametrize("name", ["cavity_disk", "channel_growth"])
+def test_graph_stepping_matches_host_stepping(name):
+    """The captured step graph (solver loops as device-terminated WHILE nodes) runs
+    exactly the kernels of host-driven stepping: states agree bit for bit."""
+    w = workloads.cavity_disk(N=32) if name == "cavity_disk" else workloads.channel_growth(N=16)
+    (ga, ra, sa), (gb, rb, sb) = _graph_vs_host(w, 4)
+    for f in ("U", "V", "phi", "resource", "sigma_xx", "sigma_yy", "sigma_xy"):
+        np.testing.assert_array_equal(getattr(ga, f), getattr(gb, f))
+    import dataclasses
+    np.testing.assert_array_equal([dataclasses.astuple(r) for r in ra], [dataclasses.astuple(r) for r in rb])
+    assert sa["projection_iterations"] == sb["projection_iterations"]
+    assert sa["velocity_iterations"] == sb["velocity_iterations"]
+    assert sa["kernel_launches"] > 0
+
+
+def test_step_n_matches_single_steps_and_reports_failing_step():
+    w = workloads.cavity_disk(N=16)
+    gpu, _ = pair(w.metrics, w.bcs, w.models, w.numerics)
+    st1 = w.state.copy()
+    gpu.upload(st1)
+    gpu.set_correction(fz(16, 16))
+    for k in range(3):
+        gpu.call("integrate_step", k * w.dt, w.dt, None)
+    gpu.download(st1)
+    st2 = w.state.copy()
+    gpu.upload(st2)
+    gpu.set_correction(fz(16, 16))
+    dts = (C.c_double * 3)(*([w.dt] * 3))
+    gpu.call("step_n", 0.0, dts, 3, None)
+    gpu.download(st2)
+    np.testing.assert_array_equal(st1.U, st2.U)
+    np.testing.assert_array_equal(st1.phi, st2.phi)
+    # a step size that is not positive is rejected before anything runs
+    bad = (C.c_double * 3)(w.dt, -1.0, w.dt)
+    with pytest.raises(ef.ArgumentError):
+        gpu.call("step_n", 0.0, bad, 3, None)
+    # a state that fails stage 1 stops the batch at step 1 and commits nothing
+    st3 = st2.copy()
+    st3.U[5, 5] += 0.5
+    gpu.upload(st3)
+    with pytest.raises(ef.ArgumentError, match="step 1 of 3"):
+        gpu.call("step_n", 0.0, dts, 3, None)
+    after = st3.copy()
+    gpu.download(after)
+    np.testing.assert_array_equal(after.U, st3.U)
