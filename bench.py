@@ -268,7 +268,7 @@ def main():
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     p.add_argument("--projection-reltol", type=float, default=1e-10)
     p.add_argument("--velocity-reltol", type=float, default=1e-8)
-    p.add_argument("--site", default="pcg_update")
+    p.add_argument("--site", default="visc_cg")
     p.add_argument("--traffic", type=float, default=None, help="ncu dram bytes per launch of the site")
     p.add_argument("--site-steps", type=int, default=3)
     p.add_argument("--e2e-steps", type=int, default=5)

@@ -114,7 +114,7 @@ class Stats(Structure):
                 ("site_bytes", c_double)]
 
 
-SITES = ["phase", "momentum", "structure", "visc_apply", "visc_matvec", "visc_update", "pcg_matvec",
+SITES = ["phase", "momentum", "structure", "visc_apply", "visc_cg", "visc_init", "pcg_matvec",
          "pcg_update", "vcycle", "proj_rhs", "proj_finish", "combine", "vel_rhs", "finalize"]
 
 

@@ -438,6 +438,7 @@ void build_projection(efsi_handle* h, const efsi_config& cfg) {
         throw Err{EFSI_UNSUPPORTED, "the projection multigrid needs grid sizes that halve down to at most 1024 coarse cells"};
     const double ax = h->P.g.hy / h->P.g.hx, ay = h->P.g.hx / h->P.g.hy;
     pj.nlev = (int)lv.size();
+    pj.nsm = h->P.nsm;
     for (int l = 0; l < pj.nlev; ++l) {
         MGLevel& M = pj.lev[l];
         const HostLevel& H = lv[l];
@@ -457,7 +458,7 @@ void build_projection(efsi_handle* h, const efsi_config& cfg) {
     pj.coarse_inv = h->dalloc<double>(inv.size());
     check_cuda(cudaMemcpy(pj.coarse_inv, inv.data(), sizeof(double) * inv.size(), cudaMemcpyHostToDevice), "mg upload");
     const size_t N = (size_t)Nx * Ny;
-    pj.x = h->dalloc<double>(N); pj.r = h->dalloc<double>(N); pj.z = pj.lev[0].xo;
+    pj.x = h->dalloc<double>(N); pj.r[0] = h->dalloc<double>(N); pj.r[1] = h->dalloc<double>(N); pj.z = pj.lev[0].xo;
     pj.p[0] = h->dalloc<double>(N); pj.p[1] = h->dalloc<double>(N);
     pj.Ap = h->dalloc<double>(N); pj.b = h->dalloc<double>(N); pj.rhs = h->dalloc<double>(N);
     pj.Up = h->dalloc<double>(h->nu); pj.Vp = h->dalloc<double>(h->nv);
@@ -612,19 +613,6 @@ void solve(efsi_handle* h, int kind, int stage, CGScal* cg, int maxiter, int ker
     h->pred[kind] = std::max(1, flags[0]);
 }
 
-// Algorithmic bytes (unique FP64 reads + writes once) of one V-cycle.
-double vcycle_bytes(const Projection& pj) {
-    double b = 0.0;
-    for (int l = 0; l + 1 < pj.nlev; ++l) {
-        double n = (double)pj.lev[l].nx * pj.lev[l].ny, nc = (double)pj.lev[l + 1].nx * pj.lev[l + 1].ny;
-        b += 10.5 * n + 2.0 * nc;
-    }
-    double nc = pj.nc;
-    return 8.0 * (b + nc * nc + 2.0 * nc);
-}
-
-int vcycle_kernels(const Projection& pj) { return 5 * (pj.nlev - 1) + 1 + (pj.nlev == 1 ? 1 : 0); }
-
 // One projection of (compact predictor | full arrays) onto div = G, writing U_out/V_out/q.
 void projection(efsi_handle* h, bool compact, const double* u_in, const double* v_in, const double* G, double* U_out,
                 double* V_out, int stage_slot) {
@@ -633,22 +621,22 @@ void projection(efsi_handle* h, bool compact, const double* u_in, const double* 
     const double N = (double)h->nc, nuv = (double)(h->nu + h->nv), g = G ? 1.0 : 0.0;
     site(h, EFSI_SITE_PROJ_RHS, 8.0 * (2.0 * nuv + N * (2.0 + g)),
          [&] { proj_rhs(P, h->pj, compact, u_in, v_in, G, &d->ps, h->slot[0], &d->st, h->stream); });
-    const double vb = vcycle_bytes(h->pj);
-    const int vk = vcycle_kernels(h->pj);
+    const double vb = proj_update_vcycle_bytes(h->pj);
+    const int vk = proj_update_vcycle_kernels(h->pj);
     solve(
-        h, KIND_PROJ, stage_slot, &d->cg_proj, P.nu.projection_maxiter, 2 * (2 + vk), 2,
+        h, KIND_PROJ, stage_slot, &d->cg_proj, P.nu.projection_maxiter, 2 * (1 + vk), 2,
         [&](cudaStream_t s, int* io, cudaGraphConditionalHandle ch) {
             proj_cg_init(P, h->pj, P.nu.projection_reltol, P.nu.projection_maxiter, h->q, &d->cg_proj, &d->ps,
                          h->slot[1], h->slot[2], &d->st, io, ch, s);
-            h->launches += 1 + vk;
+            h->launches += proj_init_kernels(h->pj);
         },
         [&](cudaStream_t s, int* io, cudaGraphConditionalHandle ch) {
             for (int par = 0; par < 2; ++par) {
                 site(h, EFSI_SITE_PCG_MATVEC, 8.0 * N * 4.0,
                      [&] { proj_matvec(P, h->pj, par, &d->cg_proj, h->slot[3], s); });
-                site(h, EFSI_SITE_PCG_UPDATE, 8.0 * N * 6.0,
-                     [&] { proj_update(P, h->pj, par, &d->cg_proj, h->slot[4], io, ch, s); });
-                site(h, EFSI_SITE_VCYCLE, vb, [&] { proj_vcycle(P, h->pj, &d->cg_proj, h->slot[5], s); });
+                site(h, EFSI_SITE_VCYCLE, vb, [&] {
+                    proj_update_vcycle(P, h->pj, par, &d->cg_proj, h->slot[4], h->slot[5], io, ch, s);
+                });
             }
         });
     site(h, EFSI_SITE_PROJ_FINISH, 8.0 * (4.0 * N + 2.0 * nuv + g * N), [&] {
@@ -751,21 +739,19 @@ void enqueue_step(efsi_handle* h) {
                 DtCoef alpha{dtp, c_AI_diag[st]};
                 const int maxit = std::max(1, P.nu.linear_maxiter);
                 solve(
-                    h, KIND_VISC, st, &d->cg_visc, maxit, 6, 2,
+                    h, KIND_VISC, st, &d->cg_visc, maxit, 2, 2,
                     [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
-                        visc_init(P, alpha, P.nu.linear_reltol, maxit, h->U, h->V, h->rhs_u, h->rhs_v, h->phis,
-                                  h->vs, &d->cg_visc, h->slot[0], io, ch, ss);
-                        h->launches += 2;
+                        site(h, EFSI_SITE_VISC_INIT, 8.0 * N * 18.0, [&] {
+                            visc_init(P, alpha, P.nu.linear_reltol, maxit, h->U, h->V, h->rhs_u, h->rhs_v, h->phis,
+                                      h->vs, &d->cg_visc, h->slot[0], h->slot[1], io, ch, ss);
+                        });
+                        h->launches += 3;
                     },
                     [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
-                        for (int k = 0; k < 2; ++k) {
-                            site(h, EFSI_SITE_VISC_MATVEC, 8.0 * N * 12.0, [&] {
-                                visc_matvec(P, alpha, h->phis, h->vs, &d->cg_visc, h->slot[1], ss);
+                        for (int k = 0; k < 2; ++k)
+                            site(h, EFSI_SITE_VISC_CG, 8.0 * N * 22.0, [&] {
+                                visc_iter(P, alpha, h->phis, h->vs, k, &d->cg_visc, h->slot[2], io, ch, ss);
                             });
-                            site(h, EFSI_SITE_VISC_UPDATE, 8.0 * N * 14.0, [&] {
-                                visc_update(P, h->vs, &d->cg_visc, h->slot[2], io, ch, ss);
-                            });
-                        }
                     });
             } else {
                 visc_enforce_dirichlet(P, h->rhs_u, h->rhs_v, h->vs.x_u, h->vs.x_v, s);
@@ -961,6 +947,7 @@ int efsi_create(const efsi_config* cfg, efsi_handle** out) {
         check_cuda(cudaEventCreate(&h->call_ev[0]), "event");
         check_cuda(cudaEventCreate(&h->call_ev[1]), "event");
         Params& P = h->P;
+        check_cuda(cudaDeviceGetAttribute(&P.nsm, cudaDevAttrMultiProcessorCount, h->device), "device attribute");
         P.g = GridD{m.Nx, m.Ny, m.periodic_x ? 1 : 0, m.periodic_y ? 1 : 0, hx, hy, 1.0 / hx, 1.0 / hy, m.Lx, m.Ly};
         const int Nx = m.Nx, Ny = m.Ny;
         upload_bcs(h.get(), cfg->bc_U, Ny, Nx + 1, P.bu, "U");
@@ -1022,10 +1009,13 @@ int efsi_create(const efsi_config* cfg, efsi_handle** out) {
         }
         ViscSolve& vs = h->vs;
         vs.x_u = h->dalloc<double>(N); vs.x_v = h->dalloc<double>(N);
-        vs.r_u = h->dalloc<double>(N); vs.r_v = h->dalloc<double>(N);
-        for (int k = 0; k < 2; ++k) { vs.p_u[k] = h->dalloc<double>(N); vs.p_v[k] = h->dalloc<double>(N); }
-        vs.Ap_u = h->dalloc<double>(N); vs.Ap_v = h->dalloc<double>(N);
+        vs.p_u = h->dalloc<double>(N); vs.p_v = h->dalloc<double>(N);
         vs.dinv_u = h->dalloc<double>(N); vs.dinv_v = h->dalloc<double>(N);
+        for (int k = 0; k < 2; ++k) {
+            vs.r_u[k] = h->dalloc<double>(N); vs.r_v[k] = h->dalloc<double>(N);
+            vs.w_u[k] = h->dalloc<double>(N); vs.w_v[k] = h->dalloc<double>(N);
+            vs.s_u[k] = h->dalloc<double>(N); vs.s_v[k] = h->dalloc<double>(N);
+        }
         ScalarSolve& ds = h->ds;
         ds.x = h->cs; ds.r = h->dalloc<double>(N);
         ds.p[0] = h->dalloc<double>(N); ds.p[1] = h->dalloc<double>(N); ds.Ap = h->dalloc<double>(N);

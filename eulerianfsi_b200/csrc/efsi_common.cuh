@@ -51,7 +51,14 @@ struct Params {
     efsi_models md;
     efsi_numerics nu;
     double psi_bc[4];  // ACDI: psi of the scalar Dirichlet phase data per side (PhaseFieldMethods.jl:509-516)
+    int nsm;           // multiprocessors of the device (persistent launch grids)
 };
+
+// Grid of a persistent (grid-stride over tiles) launch: at most `per_sm` blocks per SM.
+inline int persistent_grid(int ntiles, int nsm, int per_sm) {
+    int cap = (nsm > 0 ? nsm : 148) * per_sm;
+    return ntiles < 1 ? 1 : (ntiles < cap ? ntiles : cap);
+}
 
 // ---- device error flags ---------------------------------------------------------------
 // First error wins; the host maps `code` to an EFSI_* status and a message.
@@ -103,6 +110,8 @@ __device__ __forceinline__ void set_loop(cudaGraphConditionalHandle h, bool keep
 
 // ---- indexing ------------------------------------------------------------------------------
 __device__ __forceinline__ int wrapi(int k, int n) { return k < 0 ? k + n : (k >= n ? k - n : k); }
+// any k (tile halos may reach several periods past a small level)
+__device__ __forceinline__ int wrapm(int k, int n) { int m = k % n; return m < 0 ? m + n : m; }
 __device__ __forceinline__ size_t cidx(int i, int j, int Nx) { return (size_t)i + (size_t)j * Nx; }
 __device__ __forceinline__ size_t uidx(int i, int j, int Nx) { return (size_t)i + (size_t)j * (Nx + 1); }
 __device__ __forceinline__ size_t vidx(int i, int j, int Nx) { return (size_t)i + (size_t)j * Nx; }

@@ -42,30 +42,36 @@ struct CompactUV {
 };
 
 // Matrix part of the viscous operator (no boundary data), rows u(i,j) and v(i,j).
-template <class X>
-__device__ void visc_A(const Params& P, const MuField& mu, const X& x, int i, int j, double& au, double& av) {
+// INT: (i,j) is at least one cell away from every edge, so no boundary branch is
+// taken (the same arithmetic as the general path there, without its tests).
+template <bool INT, class X>
+__device__ __forceinline__ void visc_A(const Params& P, const MuField& mu, const X& x, int i, int j, double& au,
+                                       double& av) {
     const int Nx = P.g.Nx, Ny = P.g.Ny;
     const double ihx = P.g.ihx, ihy = P.g.ihy;
     const bool px = P.g.px, py = P.g.py;
     auto txx = [&](int c, int r) {
-        double nxt = c < Nx - 1 ? x.U(c + 1, r) : (px ? x.U(0, r) : 0.0);
+        double nxt = (INT || c < Nx - 1) ? x.U(c + 1, r) : (px ? x.U(0, r) : 0.0);
         return 2.0 * mu.c(c, r) * ((nxt - x.U(c, r)) * ihx);
     };
     auto tyy = [&](int c, int r) {
-        double nxt = r < Ny - 1 ? x.V(c, r + 1) : (py ? x.V(c, 0) : 0.0);
+        double nxt = (INT || r < Ny - 1) ? x.V(c, r + 1) : (py ? x.V(c, 0) : 0.0);
         return 2.0 * mu.c(c, r) * ((nxt - x.V(c, r)) * ihy);
     };
     auto txy = [&](int c, int r) {
-        double duy = r > 0 ? (x.U(c, r) - x.U(c, r - 1)) * ihy : (py ? (x.U(c, 0) - x.U(c, Ny - 1)) * ihy : 0.0);
-        double dvx = c > 0 ? (x.V(c, r) - x.V(c - 1, r)) * ihx : (px ? (x.V(0, r) - x.V(Nx - 1, r)) * ihx : 0.0);
+        double duy = (INT || r > 0) ? (x.U(c, r) - x.U(c, r - 1)) * ihy
+                                    : (py ? (x.U(c, 0) - x.U(c, Ny - 1)) * ihy : 0.0);
+        double dvx = (INT || c > 0) ? (x.V(c, r) - x.V(c - 1, r)) * ihx
+                                    : (px ? (x.V(0, r) - x.V(Nx - 1, r)) * ihx : 0.0);
         return 2.0 * mu.k(c, r) * (0.5 * duy + 0.5 * dvx);
     };
-    double axx = txx(i, j) - (i > 0 ? txx(i - 1, j) : (px ? txx(Nx - 1, j) : 0.0));
-    double axy = -txy(i, j) + (j < Ny - 1 ? txy(i, j + 1) : (py ? txy(i, 0) : 0.0));
+    double axx = txx(i, j) - ((INT || i > 0) ? txx(i - 1, j) : (px ? txx(Nx - 1, j) : 0.0));
+    double axy = -txy(i, j) + ((INT || j < Ny - 1) ? txy(i, j + 1) : (py ? txy(i, 0) : 0.0));
     au = axx * ihx + axy * ihy;
-    double ayx = -txy(i, j) + (i < Nx - 1 ? txy(i + 1, j) : (px ? txy(0, j) : 0.0));
-    double ayy = tyy(i, j) - (j > 0 ? tyy(i, j - 1) : (py ? tyy(i, Ny - 1) : 0.0));
+    double ayx = -txy(i, j) + ((INT || i < Nx - 1) ? txy(i + 1, j) : (px ? txy(0, j) : 0.0));
+    double ayy = tyy(i, j) - ((INT || j > 0) ? tyy(i, j - 1) : (py ? tyy(i, Ny - 1) : 0.0));
     av = ayx * ihx + ayy * ihy;
+    if (INT) return;
     if (!py) {
         if (j == 0 && P.bu.s[BOTTOM].type == EFSI_BC_DIRICHLET) au -= mu.k(i, 0) / (P.g.hy * (0.5 * P.g.hy)) * x.U(i, 0);
         if (j == Ny - 1 && P.bu.s[TOP].type == EFSI_BC_DIRICHLET)
@@ -76,6 +82,12 @@ __device__ void visc_A(const Params& P, const MuField& mu, const X& x, int i, in
         if (i == Nx - 1 && P.bv.s[RIGHT].type == EFSI_BC_DIRICHLET)
             av -= mu.k(Nx, j) / (P.g.hx * (0.5 * P.g.hx)) * x.V(Nx - 1, j);
     }
+}
+template <class X>
+__device__ __forceinline__ void visc_A_any(const Params& P, const MuField& mu, const X& x, int i, int j, double& au,
+                                           double& av) {
+    if (i >= 1 && i <= P.g.Nx - 2 && j >= 1 && j <= P.g.Ny - 2) visc_A<true>(P, mu, x, i, j, au, av);
+    else visc_A<false>(P, mu, x, i, j, au, av);
 }
 
 // Diagonal of the viscous operator A at rows u(i,j), v(i,j).
@@ -133,7 +145,7 @@ __global__ void k_visc_init(Params P, DtCoef ac, double reltol, int maxiter, con
         MuField mu = make_mu(P, phi);
         CompactUV x{xu, xv, Nx};
         double au, av, du, dv;
-        visc_A(P, mu, x, i, j, au, av);
+        visc_A_any(P, mu, x, i, j, au, av);
         visc_diag(P, mu, i, j, du, dv);
         size_t k = cidx(i, j, Nx);
         double r1 = u_fixed(P, i) ? 0.0 : rhs_u[k] - (xu[k] - alpha * au);
@@ -151,10 +163,11 @@ __global__ void k_visc_init(Params P, DtCoef ac, double reltol, int maxiter, con
     if (grid_reduce<2>(acc, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0) {
         cg->rr0 = tot[0];
         cg->rr = tot[0];
-        cg->rz = tot[1];
+        cg->rz = tot[1];  // gamma_0 = r.M r
         cg->tol2 = reltol * reltol * tot[0];
         cg->iter = 0;
         cg->maxiter = maxiter;
+        cg->alpha = 0.0;
         cg->beta = 0.0;
         cg->conv = tot[0] == 0.0 ? 1 : 0;
         cg->done = (cg->conv || !isfinite(tot[0])) ? 1 : 0;  // a non-finite start ends at once
@@ -163,104 +176,235 @@ __global__ void k_visc_init(Params P, DtCoef ac, double reltol, int maxiter, con
     }
 }
 
-// p = D^-1 r + beta*p (Jacobi-preconditioned search direction; zero on Dirichlet rows).
-__global__ void k_visc_pupdate(int n, const double* __restrict__ ru, const double* __restrict__ rv,
-                               const double* __restrict__ dinv_u, const double* __restrict__ dinv_v, double* pu,
-                               double* pv, const CGScal* cg) {
-    if (cg->done) return;
-    const int first = cg->iter == 0;
-    const double beta = first ? 0.0 : cg->beta;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        double a = ru[k] * dinv_u[k], b = rv[k] * dinv_v[k];
-        pu[k] = first ? a : a + beta * pu[k];
-        pv[k] = first ? b : b + beta * pv[k];
+// ---- Chronopoulos-Gear CG, one kernel per iteration ------------------------------------
+// With u = M r (Jacobi) and w = A u, one iteration i -> i+1 is
+//   p_i = u_i + b_i p_{i-1},  s_i = w_i + b_i s_{i-1},  x += a_i p_i,  r_{i+1} = r_i - a_i s_i,
+//   u_{i+1} = M r_{i+1},  w_{i+1} = A u_{i+1},
+//   g = r_{i+1}.u_{i+1},  d = u_{i+1}.w_{i+1},  b_{i+1} = g / g_i,  a_{i+1} = g / (d - b_{i+1} g / a_i),
+// so the three dot products (g, d, |r|^2) share one grid reduction.  In exact
+// arithmetic this is the Jacobi-PCG of the reference's SPD system; u_{i+1} is
+// staged in shared memory over the block's tile plus a one-cell halo.
+constexpr int VTX = 32, VTY = 8, VSX = VTX + 2, VSY = VTY + 2;
+
+// Shared-memory view of a compact (u, v) pair over one tile with a one-cell halo.
+// Slots hold the values at wrapped global indices (periodic) or zero outside walls;
+// requests use global indices, wrapped requests are mapped back into the halo.
+struct TileUV {
+    const double* su;
+    const double* sv;
+    int i0, j0, Nx, Ny;
+    __device__ __forceinline__ int slot(int c, int r) const {
+        int lc = c - i0 + 1, lr = r - j0 + 1;
+        if (lc < 0) lc += Nx; else if (lc >= VSX) lc -= Nx;
+        if (lr < 0) lr += Ny; else if (lr >= VSY) lr -= Ny;
+        return lr * VSX + lc;
+    }
+    __device__ __forceinline__ double U(int c, int r) const { return su[slot(c, r)]; }
+    __device__ __forceinline__ double V(int c, int r) const { return sv[slot(c, r)]; }
+};
+
+struct ViscIterArgs {
+    const double *r_u, *r_v, *w_u, *w_v, *s_u, *s_v;  // iteration i (read)
+    double *rn_u, *rn_v, *wn_u, *wn_v, *sn_u, *sn_v;  // iteration i+1 (written)
+    double *x_u, *x_v, *p_u, *p_v;
+    const double *dinv_u, *dinv_v;
+};
+
+// Global index of halo slot h (0 <= h < 2*VSX + 2*VTY) of a tile.
+__device__ __forceinline__ void visc_halo_slot(int h, int& lx, int& ly) {
+    if (h < VSX) { lx = h; ly = 0; }
+    else if (h < 2 * VSX) { lx = h - VSX; ly = VSY - 1; }
+    else { int t = h - 2 * VSX; lx = t < VTY ? 0 : VSX - 1; ly = 1 + (t % VTY); }
+}
+
+// w = u - alpha*A u at the thread's own point from the staged tile (0 on Dirichlet rows).
+__device__ __forceinline__ void visc_apply_tile(const Params& P, double alpha, const double* phi, const TileUV& t,
+                                                int i, int j, double un, double vn, double& w1, double& w2) {
+    MuField mu = make_mu(P, phi);
+    double au, av;
+    visc_A_any(P, mu, t, i, j, au, av);
+    w1 = u_fixed(P, i) ? 0.0 : un - alpha * au;
+    w2 = v_fixed(P, j) ? 0.0 : vn - alpha * av;
+}
+
+// Staged value u = M r (INIT) or u_{i+1} = M (r_i - a (w_i + b s_{i-1})) at (gi, gj);
+// zero outside walls, wrapped when periodic.
+template <bool INIT>
+__device__ __forceinline__ void visc_stage_value(const Params& P, const ViscIterArgs& v, bool first, double a,
+                                                 double b, int gi, int gj, double& hu, double& hv) {
+    const int Nx = P.g.Nx, Ny = P.g.Ny;
+    const bool inx = gi >= 0 && gi < Nx, iny = gj >= 0 && gj < Ny;
+    hu = 0.0;
+    hv = 0.0;
+    if (!((inx || P.g.px) && (iny || P.g.py))) return;
+    const size_t k = cidx(inx ? gi : wrapm(gi, Nx), iny ? gj : wrapm(gj, Ny), Nx);
+    if (INIT) {
+        hu = v.dinv_u[k] * v.r_u[k];
+        hv = v.dinv_v[k] * v.r_v[k];
+    } else {
+        double s1 = first ? v.w_u[k] : v.w_u[k] + b * v.s_u[k];
+        double s2 = first ? v.w_v[k] : v.w_v[k] + b * v.s_v[k];
+        hu = v.dinv_u[k] * (v.r_u[k] - a * s1);
+        hv = v.dinv_v[k] * (v.r_v[k] - a * s2);
     }
 }
 
-// Ap = (I - alpha*A) p on the free rows (0 on Dirichlet rows), partial p.Ap -> alpha_cg.
-__global__ void k_visc_matvec(Params P, DtCoef ac, const double* __restrict__ phi, const double* __restrict__ pu,
-                              const double* __restrict__ pv, double* Apu, double* Apv, CGScal* cg, RedSlot rs) {
+// w_0 = A M r_0 and d_0 = u_0.w_0 -> a_0 = g_0 / d_0.
+__global__ void __launch_bounds__(VTX * VTY, 4) k_visc_w0(Params P, DtCoef ac, const double* __restrict__ phi,
+                                                          ViscIterArgs v, CGScal* cg, RedSlot rs) {
+    __shared__ double su[VSX * VSY], sv[VSX * VSY];
     __shared__ double sh[32];
     if (cg->done) return;
     const double alpha = ac.value();
-    const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
-    const int Nx = P.g.Nx, Ny = P.g.Ny;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + ty * VTX;
+    const int ntx = (P.g.Nx + VTX - 1) / VTX, nt = ntx * ((P.g.Ny + VTY - 1) / VTY);
     double acc[1] = {0.0};
-    if (i < Nx && j < Ny) {
-        MuField mu = make_mu(P, phi);
-        CompactUV x{pu, pv, Nx};
-        size_t k = cidx(i, j, Nx);
-        double au, av;
-        visc_A(P, mu, x, i, j, au, av);
-        double a = pu[k], b = pv[k];
-        double qa = u_fixed(P, i) ? 0.0 : a - alpha * au;
-        double qb = v_fixed(P, j) ? 0.0 : b - alpha * av;
-        Apu[k] = qa; Apv[k] = qb;
-        acc[0] = a * qa + b * qb;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int i0 = (t % ntx) * VTX, j0 = (t / ntx) * VTY;
+        const int i = i0 + tx, j = j0 + ty;
+        double un, vn;
+        visc_stage_value<true>(P, v, true, 0.0, 0.0, i, j, un, vn);
+        su[(ty + 1) * VSX + tx + 1] = un;
+        sv[(ty + 1) * VSX + tx + 1] = vn;
+        if (tid < 2 * VSX + 2 * VTY) {
+            int lx, ly;
+            visc_halo_slot(tid, lx, ly);
+            double hu, hv;
+            visc_stage_value<true>(P, v, true, 0.0, 0.0, i0 + lx - 1, j0 + ly - 1, hu, hv);
+            su[ly * VSX + lx] = hu;
+            sv[ly * VSX + lx] = hv;
+        }
+        __syncthreads();
+        if (i < P.g.Nx && j < P.g.Ny) {
+            TileUV tl{su, sv, i0, j0, P.g.Nx, P.g.Ny};
+            double w1, w2;
+            visc_apply_tile(P, alpha, phi, tl, i, j, un, vn, w1, w2);
+            size_t k = cidx(i, j, P.g.Nx);
+            v.wn_u[k] = w1;
+            v.wn_v[k] = w2;
+            acc[0] += un * w1 + vn * w2;
+        }
+        __syncthreads();
     }
     double tot[1];
-    if (grid_reduce<1>(acc, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0) {
+    if (grid_reduce<1>(acc, rs, tot, sh) && tid == 0) {
         cg->pAp = tot[0];
         cg->alpha = tot[0] != 0.0 ? cg->rz / tot[0] : 0.0;
     }
 }
 
-// x += a p, r -= a Ap, partial |r|^2 and r.z  ->  convergence and beta.
-__global__ void k_visc_update(Params P, const double* __restrict__ dinv_u, const double* __restrict__ dinv_v,
-                              double* xu, double* xv, double* ru, double* rv, const double* __restrict__ pu,
-                              const double* __restrict__ pv, const double* __restrict__ Apu,
-                              const double* __restrict__ Apv, CGScal* cg, RedSlot rs, int* iters_out,
-                              cudaGraphConditionalHandle cond) {
-    __shared__ double sh[64];
+__global__ void __launch_bounds__(VTX * VTY, 4) k_visc_cg(Params P, DtCoef ac, const double* __restrict__ phi,
+                                                          ViscIterArgs v, CGScal* cg, RedSlot rs, int* iters_out,
+                                                          cudaGraphConditionalHandle cond) {
+    __shared__ double su[VSX * VSY], sv[VSX * VSY];
+    __shared__ double sh[3 * 32];
     if (cg->done) return;
-    const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
-    const int Nx = P.g.Nx;
-    const double a = cg->alpha;
-    double acc[2] = {0.0, 0.0};
-    if (i < Nx && j < P.g.Ny) {
-        size_t k = cidx(i, j, Nx);
-        xu[k] += a * pu[k];
-        xv[k] += a * pv[k];
-        double r1 = ru[k] - a * Apu[k], r2 = rv[k] - a * Apv[k];
-        ru[k] = r1; rv[k] = r2;
-        acc[0] = r1 * r1 + r2 * r2;
-        acc[1] = r1 * r1 * dinv_u[k] + r2 * r2 * dinv_v[k];
+    const double alpha = ac.value();
+    const bool first = cg->iter == 0;
+    const double a = cg->alpha, b = first ? 0.0 : cg->beta;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + ty * VTX;
+    const int Nx = P.g.Nx, Ny = P.g.Ny;
+    const int ntx = (Nx + VTX - 1) / VTX, nt = ntx * ((Ny + VTY - 1) / VTY);
+    double acc[3] = {0.0, 0.0, 0.0};  // g = r.u, d = u.w, |r|^2
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int i0 = (t % ntx) * VTX, j0 = (t / ntx) * VTY;
+        const int i = i0 + tx, j = j0 + ty;
+        const bool own = i < Nx && j < Ny;
+        double un = 0.0, vn = 0.0;
+        if (own) {
+            const size_t k = cidx(i, j, Nx);
+            const double d1 = v.dinv_u[k], d2 = v.dinv_v[k];
+            const double r1 = v.r_u[k], r2 = v.r_v[k];
+            const double s1 = first ? v.w_u[k] : v.w_u[k] + b * v.s_u[k];
+            const double s2 = first ? v.w_v[k] : v.w_v[k] + b * v.s_v[k];
+            const double p1 = first ? d1 * r1 : d1 * r1 + b * v.p_u[k];
+            const double p2 = first ? d2 * r2 : d2 * r2 + b * v.p_v[k];
+            v.p_u[k] = p1;
+            v.p_v[k] = p2;
+            v.x_u[k] += a * p1;
+            v.x_v[k] += a * p2;
+            v.sn_u[k] = s1;
+            v.sn_v[k] = s2;
+            const double q1 = r1 - a * s1, q2 = r2 - a * s2;
+            v.rn_u[k] = q1;
+            v.rn_v[k] = q2;
+            un = d1 * q1;
+            vn = d2 * q2;
+            acc[0] += q1 * un + q2 * vn;
+            acc[2] += q1 * q1 + q2 * q2;
+        } else {
+            visc_stage_value<false>(P, v, first, a, b, i, j, un, vn);
+        }
+        su[(ty + 1) * VSX + tx + 1] = un;
+        sv[(ty + 1) * VSX + tx + 1] = vn;
+        if (tid < 2 * VSX + 2 * VTY) {
+            int lx, ly;
+            visc_halo_slot(tid, lx, ly);
+            double hu, hv;
+            visc_stage_value<false>(P, v, first, a, b, i0 + lx - 1, j0 + ly - 1, hu, hv);
+            su[ly * VSX + lx] = hu;
+            sv[ly * VSX + lx] = hv;
+        }
+        __syncthreads();
+        if (own) {
+            TileUV tl{su, sv, i0, j0, Nx, Ny};
+            double w1, w2;
+            visc_apply_tile(P, alpha, phi, tl, i, j, un, vn, w1, w2);
+            const size_t k = cidx(i, j, Nx);
+            v.wn_u[k] = w1;
+            v.wn_v[k] = w2;
+            acc[1] += un * w1 + vn * w2;
+        }
+        __syncthreads();
     }
-    double tot[2];
-    if (grid_reduce<2>(acc, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0) {
+    double tot[3];
+    if (grid_reduce<3>(acc, rs, tot, sh) && tid == 0) {
+        const double g = tot[0], d = tot[1];
         cg->iter += 1;
-        cg->rr = tot[0];
-        cg->beta = cg->rz != 0.0 ? tot[1] / cg->rz : 0.0;
-        cg->rz = tot[1];
-        if (tot[0] <= cg->tol2) { cg->conv = 1; cg->done = 1; }
-        else if (cg->iter >= cg->maxiter || !isfinite(tot[0])) cg->done = 1;
+        cg->rr = tot[2];
+        const double bn = cg->rz != 0.0 ? g / cg->rz : 0.0;
+        const double den = d - (cg->alpha != 0.0 ? bn * g / cg->alpha : 0.0);
+        cg->beta = bn;
+        cg->alpha = den != 0.0 ? g / den : 0.0;
+        cg->rz = g;
+        cg->pAp = d;
+        if (tot[2] <= cg->tol2) { cg->conv = 1; cg->done = 1; }
+        else if (cg->iter >= cg->maxiter || !isfinite(tot[2])) cg->done = 1;
         if (iters_out) *iters_out = cg->iter;
         set_loop(cond, !cg->done);
     }
 }
 
-void visc_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const double* Un, const double* Vn,
-               const double* rhs_u, const double* rhs_v, const double* phi, const ViscSolve& w, CGScal* cg,
-               const RedSlot& rs, int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s) {
-    dim3 g = grid2(P.g.Nx, P.g.Ny), b(BX, BY);
-    k_visc_x0<<<g, b, 0, s>>>(P, Un, Vn, w.x_u, w.x_v);
-    k_visc_init<<<g, b, 0, s>>>(P, alpha, reltol, maxiter, w.x_u, w.x_v, rhs_u, rhs_v, phi, w.r_u, w.r_v, w.dinv_u,
-                                w.dinv_v, cg, rs, iters_out, cond);
+static ViscIterArgs visc_args(const ViscSolve& w, int parity) {
+    const int c = parity & 1, n = c ^ 1;
+    return ViscIterArgs{w.r_u[c], w.r_v[c], w.w_u[c], w.w_v[c], w.s_u[c], w.s_v[c],
+                        w.r_u[n], w.r_v[n], w.w_u[n], w.w_v[n], w.s_u[n], w.s_v[n],
+                        w.x_u, w.x_v, w.p_u, w.p_v, w.dinv_u, w.dinv_v};
 }
 
-void visc_matvec(const Params& P, DtCoef alpha, const double* phi, const ViscSolve& w, CGScal* cg, const RedSlot& rs,
-                 cudaStream_t s) {
-    const int n = P.g.Nx * P.g.Ny;
-    k_visc_pupdate<<<std::min((n + 255) / 256, 148 * 8), 256, 0, s>>>(n, w.r_u, w.r_v, w.dinv_u, w.dinv_v, w.p_u[0],
-                                                                     w.p_v[0], cg);
-    k_visc_matvec<<<grid2(P.g.Nx, P.g.Ny), dim3(BX, BY), 0, s>>>(P, alpha, phi, w.p_u[0], w.p_v[0], w.Ap_u, w.Ap_v,
-                                                              cg, rs);
+void visc_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const double* Un, const double* Vn,
+               const double* rhs_u, const double* rhs_v, const double* phi, const ViscSolve& w, CGScal* cg,
+               const RedSlot& rs, const RedSlot& rs2, int* iters_out, cudaGraphConditionalHandle cond,
+               cudaStream_t s) {
+    dim3 g = grid2(P.g.Nx, P.g.Ny), b(BX, BY);
+    k_visc_x0<<<g, b, 0, s>>>(P, Un, Vn, w.x_u, w.x_v);
+    k_visc_init<<<g, b, 0, s>>>(P, alpha, reltol, maxiter, w.x_u, w.x_v, rhs_u, rhs_v, phi, w.r_u[0], w.r_v[0],
+                                w.dinv_u, w.dinv_v, cg, rs, iters_out, cond);
+    // w_0 goes to the parity-0 "read" slot: the first iteration reads (r, w)[0].
+    ViscIterArgs v = visc_args(w, 1);
+    v.r_u = w.r_u[0];
+    v.r_v = w.r_v[0];
+    v.wn_u = w.w_u[0];
+    v.wn_v = w.w_v[0];
+    const int nt = ((P.g.Nx + VTX - 1) / VTX) * ((P.g.Ny + VTY - 1) / VTY);
+    k_visc_w0<<<persistent_grid(nt, P.nsm, 4), dim3(VTX, VTY), 0, s>>>(P, alpha, phi, v, cg, rs2);
 }
-void visc_update(const Params& P, const ViscSolve& w, CGScal* cg, const RedSlot& rs, int* iters_out,
-                 cudaGraphConditionalHandle cond, cudaStream_t s) {
-    k_visc_update<<<grid2(P.g.Nx, P.g.Ny), dim3(BX, BY), 0, s>>>(P, w.dinv_u, w.dinv_v, w.x_u, w.x_v, w.r_u, w.r_v,
-                                                              w.p_u[0], w.p_v[0], w.Ap_u, w.Ap_v, cg, rs, iters_out,
-                                                              cond);
+
+void visc_iter(const Params& P, DtCoef alpha, const double* phi, const ViscSolve& w, int parity, CGScal* cg,
+               const RedSlot& rs, int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s) {
+    const int nt = ((P.g.Nx + VTX - 1) / VTX) * ((P.g.Ny + VTY - 1) / VTY);
+    k_visc_cg<<<persistent_grid(nt, P.nsm, 4), dim3(VTX, VTY), 0, s>>>(P, alpha, phi, visc_args(w, parity), cg, rs,
+                                                                        iters_out, cond);
 }
 
 // NoViscosity: predictor = rhs with the Dirichlet rows enforced (:786-788).
@@ -470,48 +614,8 @@ __device__ __forceinline__ double lev_off(const MGLevel& L, int px, int py, int 
     if (j < L.ny - 1) off += L.ay * x(i, j + 1); else if (py) off += L.ay * x(i, 0);
     return off;
 }
-__device__ __forceinline__ bool lev_rb(const MGLevel& L, int px, int py) {
-    return !((px && (L.nx & 1)) || (py && (L.ny & 1)));  // valid red-black colouring
-}
-static constexpr double JACOBI_W = 0.8;
 
-// Pre-smoothing from x = 0: red cells x = b/D, black cells one GS update
-// (or one damped-Jacobi sweep when the periodic colouring is not bipartite).
-__global__ void k_mg_pre(MGLevel L, int px, int py, const double* __restrict__ b, double* x, const CGScal* cg) {
-    if (cg && cg->done) return;
-    const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
-    if (i >= L.nx || j >= L.ny) return;
-    const int nx = L.nx;
-    double d;
-    lev_diag(L, px, py, i, j, d);
-    double bc = b[cidx(i, j, nx)];
-    double out;
-    if (!lev_rb(L, px, py)) out = JACOBI_W * bc / d;
-    else if (((i + j) & 1) == 0) out = bc / d;
-    else {
-        auto red = [&](int a, int c) {
-            double dd;
-            lev_diag(L, px, py, a, c, dd);
-            return b[cidx(a, c, nx)] / dd;
-        };
-        out = (bc + lev_off(L, px, py, i, j, red)) / d;
-    }
-    x[cidx(i, j, nx)] = out;
-}
-
-__global__ void k_mg_resid(MGLevel L, int px, int py, const double* __restrict__ b, const double* __restrict__ x,
-                           double* r, const CGScal* cg) {
-    if (cg && cg->done) return;
-    const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
-    if (i >= L.nx || j >= L.ny) return;
-    const int nx = L.nx;
-    double d;
-    lev_diag(L, px, py, i, j, d);
-    auto xf = [&](int a, int c) { return x[cidx(a, c, nx)]; };
-    r[cidx(i, j, nx)] = b[cidx(i, j, nx)] - (d * x[cidx(i, j, nx)] - lev_off(L, px, py, i, j, xf));
-}
-
-// Restriction b_c = P^T r (bilinear weights, reflection at walls, wrap when periodic).
+// Restriction weights of coarse cell I (bilinear P^T, reflection at walls, wrap when periodic).
 __device__ __forceinline__ void rweights(int I, int nc, bool per, int (&f)[4], double (&w)[4]) {
     f[0] = 2 * I - 1; w[0] = 0.25;
     f[1] = 2 * I;     w[1] = 0.75 + ((I == 0 && !per) ? 0.25 : 0.0);
@@ -520,27 +624,6 @@ __device__ __forceinline__ void rweights(int I, int nc, bool per, int (&f)[4], d
     const int nf = 2 * nc;
     if (f[0] < 0) { if (per) f[0] += nf; else w[0] = 0.0; }
     if (f[3] >= nf) { if (per) f[3] -= nf; else w[3] = 0.0; }
-}
-__global__ void k_mg_restrict(MGLevel F, MGLevel C, int px, int py, const double* __restrict__ r, double* bc,
-                              const CGScal* cg) {
-    if (cg && cg->done) return;
-    const int I = blockIdx.x * BX + threadIdx.x, J = blockIdx.y * BY + threadIdx.y;
-    if (I >= C.nx || J >= C.ny) return;
-    int fx[4], fy[4];
-    double wx[4], wy[4];
-    rweights(I, C.nx, px, fx, wx);
-    rweights(J, C.ny, py, fy, wy);
-    double s = 0.0;
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-        if (wy[b] == 0.0) continue;
-        double row = 0.0;
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-            if (wx[a] != 0.0) row += wx[a] * r[cidx(fx[a], fy[b], F.nx)];
-        s += wy[b] * row;
-    }
-    bc[cidx(I, J, C.nx)] = s;
 }
 
 // Bilinear prolongation value (P e) at fine cell (i,j).
@@ -558,53 +641,264 @@ __device__ __forceinline__ double prolong(const MGLevel& C, int px, int py, cons
     return 0.75 * (0.75 * E(I0, J0) + 0.25 * E(I1, J0)) + 0.25 * (0.75 * E(I0, J1) + 0.25 * E(I1, J1));
 }
 
-// x_out = x + P e on red cells; black cells are smoothed against the corrected red
-// neighbours (the first half of the post-smoothing black-then-red sweep).
-__global__ void k_mg_prolong_black(MGLevel F, MGLevel C, int px, int py, const double* __restrict__ x,
-                                   const double* __restrict__ e, const double* __restrict__ b, double* xo,
-                                   const CGScal* cg) {
-    if (cg && cg->done) return;
-    const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
-    if (i >= F.nx || j >= F.ny) return;
-    const int nx = F.nx;
-    auto xc = [&](int a, int c) { return x[cidx(a, c, nx)] + prolong(C, px, py, e, a, c); };
-    double out;
-    double d;
-    lev_diag(F, px, py, i, j, d);
-    if (!lev_rb(F, px, py)) {
-        double xx = xc(i, j);
-        out = xx + JACOBI_W * (b[cidx(i, j, nx)] - (d * xx - lev_off(F, px, py, i, j, xc))) / d;
-    } else if (((i + j) & 1) == 0) {
-        out = xc(i, j);
-    } else {
-        out = (b[cidx(i, j, nx)] + lev_off(F, px, py, i, j, xc)) / d;
-    }
-    xo[cidx(i, j, nx)] = out;
+// ---- fused multigrid kernels ----------------------------------------------------------------
+// Each block owns T x T fine cells ((T/2)^2 coarse cells) per tile and loops over tiles
+// (persistent grid).  Shared-memory slots hold values at wrapped global indices when
+// periodic and zero outside walls, so a neighbour that exists (lev_off's tests) is the
+// adjacent slot.  The slot's diagonal (0 = no cell) is computed once per tile.  Red
+// cells are (i+j) even; tile origins are even, so the colour of a slot is the parity of
+// its local coordinates.  A tile whose loaded region is at least one cell away from
+// every edge is "inner": constant diagonal, all four couplings present.
+struct SlotPos {
+    int wi, wj;    // wrapped global cell
+    bool valid;    // a cell of the level (possibly through periodic wrap)
+};
+__device__ __forceinline__ SlotPos slot_pos(const MGLevel& L, int px, int py, int gi, int gj) {
+    const bool inx = gi >= 0 && gi < L.nx, iny = gj >= 0 && gj < L.ny;
+    SlotPos p;
+    p.valid = (inx || px) && (iny || py);
+    p.wi = inx ? gi : (p.valid ? wrapm(gi, L.nx) : 0);
+    p.wj = iny ? gj : (p.valid ? wrapm(gj, L.ny) : 0);
+    return p;
+}
+// lev_off over neighbour slots (W, E, S, N order); (gi, gj) unwrapped: a wrapped slot
+// lies in a periodic direction, where every coupling exists.
+__device__ __forceinline__ double slot_off(const MGLevel& L, int px, int py, int gi, int gj, const double* s, int k,
+                                           int row) {
+    double off = 0.0;
+    off += ((gi > 0 || px) ? L.ax : 0.0) * s[k - 1];
+    off += ((gi < L.nx - 1 || px) ? L.ax : 0.0) * s[k + 1];
+    off += ((gj > 0 || py) ? L.ay : 0.0) * s[k - row];
+    off += ((gj < L.ny - 1 || py) ? L.ay : 0.0) * s[k + row];
+    return off;
+}
+__device__ __forceinline__ double inner_off(const MGLevel& L, const double* s, int k, int row) {
+    double off = 0.0;
+    off += L.ax * s[k - 1];
+    off += L.ax * s[k + 1];
+    off += L.ay * s[k - row];
+    off += L.ay * s[k + row];
+    return off;
+}
+__device__ __forceinline__ double inner_diag(const MGLevel& L) {
+    double d = 0.0;
+    d += L.ax; d += L.ax; d += L.ay; d += L.ay;
+    return d;
+}
+__device__ __forceinline__ bool inner_tile(const MGLevel& L, int i0, int j0, int T, int H) {
+    return i0 - H >= 1 && i0 + T + H <= L.nx - 1 && j0 - H >= 1 && j0 + T + H <= L.ny - 1;
 }
 
-// Red half of the post-smoothing; on the fine level it also forms r.z for CG.
-__global__ void k_mg_red(MGLevel L, int px, int py, const double* __restrict__ b, double* xo, CGScal* cg,
-                         RedSlot rs, int dot) {
+// CG update fused into the finest pre-smoothing: r_new = r_old - a Kp, x += a p.
+struct CGFuse {
+    const double* r_old;
+    const double* Ap;
+    const double* p;
+    double* x;
+    double* r_new;
+};
+
+// Down leg of one level: pre-smoothing from x = 0 (red x = b/D, then one black GS
+// update), residual r = b - K x, restriction b_c = P^T r (bilinear weights, reflection
+// at walls, wrap when periodic).  Writes L.x (needed by the up leg) and C.b.
+// FUSE: b is r_new of the CG update, formed on the fly over the halo; the owned cells
+// of r_new and x are written and |r_new|^2 decides convergence.
+template <int T, bool FUSE>
+__global__ void __launch_bounds__(256, 6) k_mg_down(MGLevel L, MGLevel C, int px, int py,
+                                                    const double* __restrict__ b, CGFuse f, CGScal* cg, RedSlot rs,
+                                                    int* iters_out, cudaGraphConditionalHandle cond) {
+    constexpr int H = 3, W = T + 2 * H;
+    __shared__ double sb[W * W];  // b, then the residual (halo 1)
+    __shared__ double sx[W * W];  // pre-smoothed x (valid within halo 2)
+    __shared__ double sd[W * W];  // diagonal, 0 where there is no cell
     __shared__ double sh[32];
     if (cg && cg->done) return;
-    const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
+    const int tid = threadIdx.x;
     const int nx = L.nx;
+    const double a = FUSE ? cg->alpha : 0.0;
+    const double d0 = inner_diag(L);
     double acc[1] = {0.0};
-    const bool inside = i < L.nx && j < L.ny;
-    if (inside) {
-        double val = xo[cidx(i, j, nx)];
-        if (lev_rb(L, px, py) && ((i + j) & 1) == 0) {
-            double d;
-            lev_diag(L, px, py, i, j, d);
-            auto xf = [&](int a, int c) { return xo[cidx(a, c, nx)]; };
-            val = (b[cidx(i, j, nx)] + lev_off(L, px, py, i, j, xf)) / d;
-            xo[cidx(i, j, nx)] = val;
+    const int ntx = (nx + T - 1) / T, nt = ntx * ((L.ny + T - 1) / T);
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int bx = t % ntx, by = t / ntx;
+        const int i0 = bx * T, j0 = by * T;
+        const bool inner = inner_tile(L, i0, j0, T, H);
+        for (int s = tid; s < W * W; s += 256) {
+            const int lx = s % W, ly = s / W;
+            const int gi = i0 + lx - H, gj = j0 + ly - H;
+            double v = 0.0, d = 0.0;
+            size_t k = 0;
+            bool have = inner, own = false;
+            if (inner) {
+                k = cidx(gi, gj, nx);
+                d = d0;
+                own = lx >= H && lx < H + T && ly >= H && ly < H + T;
+            } else {
+                const SlotPos q = slot_pos(L, px, py, gi, gj);
+                have = q.valid;
+                if (have) {
+                    k = cidx(q.wi, q.wj, nx);
+                    lev_diag(L, px, py, q.wi, q.wj, d);
+                    own = gi == q.wi && gj == q.wj && lx >= H && lx < H + T && ly >= H && ly < H + T;
+                }
+            }
+            if (have) {
+                if (FUSE) {
+                    v = f.r_old[k] - a * f.Ap[k];
+                    if (own) {
+                        f.r_new[k] = v;
+                        f.x[k] += a * f.p[k];
+                        acc[0] += v * v;
+                    }
+                } else {
+                    v = b[k];
+                }
+            }
+            sb[s] = v;
+            sd[s] = d;
+            sx[s] = (have && ((lx + ly) & 1) == 0) ? v / d : 0.0;
         }
-        acc[0] = b[cidx(i, j, nx)] * val;
+        __syncthreads();
+        // black cells within halo 2
+        constexpr int B = T + 4;
+        for (int s = tid; s < B * B / 2; s += 256) {
+            const int ry = s / (B / 2), rx = 2 * (s % (B / 2)) + ((ry + 1) & 1);
+            const int lx = rx + 1, ly = ry + 1, k = ly * W + lx;
+            const double d = sd[k];
+            if (d == 0.0) continue;
+            const double off = inner ? inner_off(L, sx, k, W)
+                                     : slot_off(L, px, py, i0 + lx - H, j0 + ly - H, sx, k, W);
+            sx[k] = (sb[k] + off) / d;
+        }
+        __syncthreads();
+        // residual within halo 1 (in place of b)
+        constexpr int R = T + 2;
+        for (int s = tid; s < R * R; s += 256) {
+            const int lx = s % R + 2, ly = s / R + 2, k = ly * W + lx;
+            const double d = sd[k];
+            if (d == 0.0) continue;
+            const double off = inner ? inner_off(L, sx, k, W)
+                                     : slot_off(L, px, py, i0 + lx - H, j0 + ly - H, sx, k, W);
+            sb[k] = sb[k] - (d * sx[k] - off);
+        }
+        __syncthreads();
+        if (tid < (T / 2) * (T / 2)) {
+            // restriction: fine cells 2I-1 .. 2I+2 are slots 2(I-I0)+2 .. +5 (wrapped values
+            // already sit in the halo)
+            const int cx = tid % (T / 2), cy = tid / (T / 2);
+            const int I = bx * (T / 2) + cx, J = by * (T / 2) + cy;
+            if (I < C.nx && J < C.ny) {
+                int fx[4], fy[4];
+                double wx[4], wy[4];
+                rweights(I, C.nx, px, fx, wx);
+                rweights(J, C.ny, py, fy, wy);
+                double sum = 0.0;
+#pragma unroll
+                for (int bb = 0; bb < 4; ++bb) {
+                    if (wy[bb] == 0.0) continue;
+                    double row = 0.0;
+#pragma unroll
+                    for (int aa = 0; aa < 4; ++aa)
+                        if (wx[aa] != 0.0) row += wx[aa] * sb[(2 * cy + bb + 2) * W + 2 * cx + aa + 2];
+                    sum += wy[bb] * row;
+                }
+                C.b[cidx(I, J, C.nx)] = sum;
+            }
+        }
+        for (int s = tid; s < T * T; s += 256) {
+            const int lx = s % T, ly = s / T;
+            const int gi = i0 + lx, gj = j0 + ly;
+            if (gi < nx && gj < L.ny) L.x[cidx(gi, gj, nx)] = sx[(ly + H) * W + lx + H];
+        }
+        __syncthreads();
     }
-    if (!dot) return;
+    if (!FUSE) return;
     double tot[1];
-    if (grid_reduce<1>(acc, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0) {
+    if (grid_reduce<1>(acc, rs, tot, sh) && tid == 0) {
+        cg->iter += 1;
+        cg->rr = tot[0];
+        if (tot[0] <= cg->tol2) { cg->conv = 1; cg->done = 1; }
+        else if (cg->iter >= cg->maxiter || !isfinite(tot[0])) cg->done = 1;
+        if (iters_out) *iters_out = cg->iter;
+        set_loop(cond, !cg->done);
+    }
+}
+
+// Up leg of one level: x + P e (bilinear prolongation), then the post-smoothing
+// black-then-red Gauss-Seidel sweep; on the finest level also r.z for CG.
+template <int T, bool DOT>
+__global__ void __launch_bounds__(256, 6) k_mg_up(MGLevel L, MGLevel C, int px, int py,
+                                                  const double* __restrict__ x, const double* __restrict__ e,
+                                                  const double* __restrict__ b, double* xo, CGScal* cg, RedSlot rs) {
+    constexpr int H = 2, W = T + 2 * H;
+    __shared__ double sx[W * W];
+    __shared__ double sb[W * W];
+    __shared__ double sd[W * W];
+    __shared__ double sh[32];
+    if (cg && cg->done) return;
+    const int tid = threadIdx.x;
+    const int nx = L.nx;
+    const double d0 = inner_diag(L);
+    double acc[1] = {0.0};
+    const int ntx = (nx + T - 1) / T, nt = ntx * ((L.ny + T - 1) / T);
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int i0 = (t % ntx) * T, j0 = (t / ntx) * T;
+        const bool inner = inner_tile(L, i0, j0, T, H);
+        for (int s = tid; s < W * W; s += 256) {
+            const int lx = s % W, ly = s / W;
+            const int gi = i0 + lx - H, gj = j0 + ly - H;
+            double xv = 0.0, bv = 0.0, d = 0.0;
+            if (inner) {
+                const size_t k = cidx(gi, gj, nx);
+                xv = x[k] + prolong(C, px, py, e, gi, gj);
+                bv = b[k];
+                d = d0;
+            } else {
+                const SlotPos q = slot_pos(L, px, py, gi, gj);
+                if (q.valid) {
+                    const size_t k = cidx(q.wi, q.wj, nx);
+                    xv = x[k] + prolong(C, px, py, e, q.wi, q.wj);
+                    bv = b[k];
+                    lev_diag(L, px, py, q.wi, q.wj, d);
+                }
+            }
+            sx[s] = xv;
+            sb[s] = bv;
+            sd[s] = d;
+        }
+        __syncthreads();
+        // black cells within halo 1
+        constexpr int B = T + 2;
+        for (int s = tid; s < B * B / 2; s += 256) {
+            const int ry = s / (B / 2), rx = 2 * (s % (B / 2)) + ((ry + 1) & 1);
+            const int lx = rx + 1, ly = ry + 1, k = ly * W + lx;
+            const double d = sd[k];
+            if (d == 0.0) continue;
+            const double off = inner ? inner_off(L, sx, k, W)
+                                     : slot_off(L, px, py, i0 + lx - H, j0 + ly - H, sx, k, W);
+            sx[k] = (sb[k] + off) / d;
+        }
+        __syncthreads();
+        // red cells of the tile (their black neighbours are final); write the tile
+        for (int s = tid; s < T * T; s += 256) {
+            const int lx = s % T, ly = s / T;
+            const int gi = i0 + lx, gj = j0 + ly;
+            if (gi >= nx || gj >= L.ny) continue;
+            const int k = (ly + H) * W + lx + H;
+            const double bc = sb[k];
+            double val = sx[k];
+            if (((lx + ly) & 1) == 0) {
+                const double off = inner ? inner_off(L, sx, k, W) : slot_off(L, px, py, gi, gj, sx, k, W);
+                val = (bc + off) / sd[k];
+            }
+            xo[cidx(gi, gj, nx)] = val;
+            acc[0] += bc * val;
+        }
+        __syncthreads();
+    }
+    if (!DOT) return;
+    double tot[1];
+    if (grid_reduce<1>(acc, rs, tot, sh) && tid == 0) {
         cg->beta = cg->rz != 0.0 ? tot[0] / cg->rz : 0.0;
         cg->rz = tot[0];
     }
@@ -640,25 +934,65 @@ __global__ void k_dot_rz(int n, const double* __restrict__ r, const double* __re
     }
 }
 
-static void vcycle(const Projection& pj, int l, const double* b, double* out, CGScal* cg, const RedSlot& rs,
-                   int px, int py, cudaStream_t s) {
-    const MGLevel& L = pj.lev[l];
-    if (l == pj.nlev - 1) {
-        k_mg_dense<<<(pj.nc + 7) / 8, 256, 0, s>>>(pj.nc, pj.coarse_inv, b, out, cg);
-        if (l == 0) k_dot_rz<<<(pj.nc + 255) / 256, 256, 0, s>>>(pj.nc, b, out, cg, rs);
+// z = M r_fine with one V(1,1)-cycle; the finest down leg optionally carries the CG update.
+static void vcycle(const Projection& pj, const double* r_fine, const CGFuse* fuse, CGScal* cg, const RedSlot& rs,
+                   const RedSlot& rs2, int* iters_out, cudaGraphConditionalHandle cond, int px, int py,
+                   cudaStream_t s) {
+    const int n = pj.nlev;
+    if (n == 1) {
+        k_mg_dense<<<(pj.nc + 7) / 8, 256, 0, s>>>(pj.nc, pj.coarse_inv, r_fine, pj.z, cg);
+        k_dot_rz<<<(pj.nc + 255) / 256, 256, 0, s>>>(pj.nc, r_fine, pj.z, cg, rs2);
         return;
     }
-    const MGLevel& C = pj.lev[l + 1];
-    dim3 g = grid2(L.nx, L.ny), gc = grid2(C.nx, C.ny), bk(BX, BY);
-    k_mg_pre<<<g, bk, 0, s>>>(L, px, py, b, L.x, cg);
-    k_mg_resid<<<g, bk, 0, s>>>(L, px, py, b, L.x, L.r, cg);
-    k_mg_restrict<<<gc, bk, 0, s>>>(L, C, px, py, L.r, C.b, cg);
-    vcycle(pj, l + 1, C.b, C.xo, cg, rs, px, py, s);
-    k_mg_prolong_black<<<g, bk, 0, s>>>(L, C, px, py, L.x, C.xo, b, out, cg);
-    k_mg_red<<<g, bk, 0, s>>>(L, px, py, b, out, cg, rs, l == 0 ? 1 : 0);
+    // 32x32 tiles while they fill the device, 16x16 below (shorter dependent chains)
+    auto wide = [&](const MGLevel& L) { return ((L.nx + 31) / 32) * ((L.ny + 31) / 32) >= pj.nsm; };
+    auto grid = [&](const MGLevel& L, int T) {
+        return persistent_grid(((L.nx + T - 1) / T) * ((L.ny + T - 1) / T), pj.nsm, 6);
+    };
+    for (int l = 0; l + 1 < n; ++l) {
+        const MGLevel &L = pj.lev[l], &C = pj.lev[l + 1];
+        const double* b = l == 0 ? r_fine : L.b;
+        const bool fz = l == 0 && fuse;
+        const CGFuse fa = fz ? *fuse : CGFuse{};
+        if (wide(L)) {
+            if (fz) k_mg_down<32, true><<<grid(L, 32), 256, 0, s>>>(L, C, px, py, b, fa, cg, rs, iters_out, cond);
+            else k_mg_down<32, false><<<grid(L, 32), 256, 0, s>>>(L, C, px, py, b, fa, cg, rs, nullptr, 0);
+        } else {
+            if (fz) k_mg_down<16, true><<<grid(L, 16), 256, 0, s>>>(L, C, px, py, b, fa, cg, rs, iters_out, cond);
+            else k_mg_down<16, false><<<grid(L, 16), 256, 0, s>>>(L, C, px, py, b, fa, cg, rs, nullptr, 0);
+        }
+    }
+    const MGLevel& B = pj.lev[n - 1];
+    k_mg_dense<<<(pj.nc + 7) / 8, 256, 0, s>>>(pj.nc, pj.coarse_inv, B.b, B.xo, cg);
+    for (int l = n - 2; l >= 0; --l) {
+        const MGLevel &L = pj.lev[l], &C = pj.lev[l + 1];
+        const double* b = l == 0 ? r_fine : L.b;
+        double* out = l == 0 ? pj.z : L.xo;
+        if (wide(L)) {
+            if (l == 0) k_mg_up<32, true><<<grid(L, 32), 256, 0, s>>>(L, C, px, py, L.x, C.xo, b, out, cg, rs2);
+            else k_mg_up<32, false><<<grid(L, 32), 256, 0, s>>>(L, C, px, py, L.x, C.xo, b, out, cg, rs2);
+        } else {
+            if (l == 0) k_mg_up<16, true><<<grid(L, 16), 256, 0, s>>>(L, C, px, py, L.x, C.xo, b, out, cg, rs2);
+            else k_mg_up<16, false><<<grid(L, 16), 256, 0, s>>>(L, C, px, py, L.x, C.xo, b, out, cg, rs2);
+        }
+    }
 }
 
-int proj_kernels_per_iter(const Projection& pj) { return 2 + 6 * (pj.nlev - 1) + 1; }
+int proj_update_vcycle_kernels(const Projection& pj) { return pj.nlev == 1 ? 3 : 2 * (pj.nlev - 1) + 1; }
+int proj_init_kernels(const Projection& pj) { return 1 + (pj.nlev == 1 ? 2 : 2 * (pj.nlev - 1) + 1); }
+double proj_update_vcycle_bytes(const Projection& pj) {
+    double w = 0.0;
+    const double n0 = (double)pj.lev[0].nx * pj.lev[0].ny;
+    if (pj.nlev == 1) {
+        w = 6.0 * n0 + (double)pj.nc * pj.nc + 4.0 * pj.nc;
+    } else {
+        // finest: r_old, Kp, p, x read; x, r_new, L.x written; C.b; up: L.x, e, r_new read, z written
+        w = 10.5 * n0;
+        for (int l = 1; l + 1 < pj.nlev; ++l) w += 5.5 * (double)pj.lev[l].nx * pj.lev[l].ny;
+        w += (double)pj.nc * pj.nc + 2.0 * pj.nc;
+    }
+    return 8.0 * w;
+}
 
 // ---- right-hand side (Projection.jl:198-221) -----------------------------------------------
 __device__ __forceinline__ double q_boundary_vec(const Params& P, int i, int j) {
@@ -775,28 +1109,42 @@ __global__ void k_pcg_init(MGLevel L, int px, int py, double reltol, int maxiter
     }
 }
 
-__global__ void k_pcg_matvec(MGLevel L, int px, int py, const double* __restrict__ z,
-                             const double* __restrict__ p_old, double* p, double* Ap, CGScal* cg, RedSlot rs) {
+// p = z + beta p_old, Kp, p.Kp -> alpha.  Persistent over 32x8 tiles; cells away from
+// the edges take the branch-free form of lev_diag/lev_off (same terms, same order).
+__global__ void __launch_bounds__(BX * BY, 6) k_pcg_matvec(MGLevel L, int px, int py, const double* __restrict__ z,
+                                                           const double* __restrict__ p_old, double* p, double* Ap,
+                                                           CGScal* cg, RedSlot rs) {
     __shared__ double sh[32];
     if (cg->done) return;
     const int first = cg->iter == 0;
-    const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
-    const int nx = L.nx;
+    const int nx = L.nx, ny = L.ny;
     const double beta = first ? 0.0 : cg->beta;
-    auto pn = [&](int a, int c) {
-        size_t k = cidx(a, c, nx);
-        return first ? z[k] : z[k] + beta * p_old[k];
-    };
+    auto pn = [&](size_t k) { return first ? z[k] : z[k] + beta * p_old[k]; };
+    const int ntx = (nx + BX - 1) / BX, nt = ntx * ((ny + BY - 1) / BY);
     double acc[1] = {0.0};
-    if (i < L.nx && j < L.ny) {
-        double d;
-        lev_diag(L, px, py, i, j, d);
-        double pc = pn(i, j);
-        double q = d * pc - lev_off(L, px, py, i, j, pn);
-        size_t k = cidx(i, j, nx);
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int i = (t % ntx) * BX + threadIdx.x, j = (t / ntx) * BY + threadIdx.y;
+        if (i >= nx || j >= ny) continue;
+        const size_t k = cidx(i, j, nx);
+        const double pc = pn(k);
+        double q;
+        if (i > 0 && i < nx - 1 && j > 0 && j < ny - 1) {
+            double d = 0.0;
+            d += L.ax; d += L.ax; d += L.ay; d += L.ay;
+            double off = 0.0;
+            off += L.ax * pn(k - 1);
+            off += L.ax * pn(k + 1);
+            off += L.ay * pn(k - nx);
+            off += L.ay * pn(k + nx);
+            q = d * pc - off;
+        } else {
+            double d;
+            lev_diag(L, px, py, i, j, d);
+            q = d * pc - lev_off(L, px, py, i, j, [&](int a, int c) { return pn(cidx(a, c, nx)); });
+        }
         p[k] = pc;
         Ap[k] = q;
-        acc[0] = pc * q;
+        acc[0] += pc * q;
     }
     double tot[1];
     if (grid_reduce<1>(acc, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0) {
@@ -835,26 +1183,32 @@ void proj_cg_init(const Params& P, const Projection& pj, double reltol, int maxi
                   const ProjScal* ps, const RedSlot& rs, const RedSlot& rs2, const DevStatus* st, int* iters_out,
                   cudaGraphConditionalHandle cond, cudaStream_t s) {
     const MGLevel& L = pj.lev[0];
-    k_pcg_init<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, s>>>(L, P.g.px, P.g.py, reltol, maxiter, q0, pj.b, pj.x, pj.r,
-                                                          ps, cg, rs, st, iters_out, cond);
-    vcycle(pj, 0, pj.r, pj.z, cg, rs2, P.g.px, P.g.py, s);
+    k_pcg_init<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, s>>>(L, P.g.px, P.g.py, reltol, maxiter, q0, pj.b, pj.x,
+                                                          pj.r[0], ps, cg, rs, st, iters_out, cond);
+    vcycle(pj, pj.r[0], nullptr, cg, rs, rs2, nullptr, 0, P.g.px, P.g.py, s);
 }
 
-// One CG iteration; `parity` selects the search-direction buffers (p[parity] is written).
+// One CG iteration is proj_matvec then proj_update_vcycle with the same parity:
+// p[parity] is written, r[parity] is read and r[parity^1] written (multigrid case).
 void proj_matvec(const Params& P, const Projection& pj, int parity, CGScal* cg, const RedSlot& rs, cudaStream_t s) {
     const MGLevel& L = pj.lev[0];
     const int cur = parity & 1, old = cur ^ 1;
-    k_pcg_matvec<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, s>>>(L, P.g.px, P.g.py, pj.z, pj.p[old], pj.p[cur], pj.Ap, cg,
-                                                            rs);
+    const int nt = ((L.nx + BX - 1) / BX) * ((L.ny + BY - 1) / BY);
+    k_pcg_matvec<<<persistent_grid(nt, pj.nsm, 6), dim3(BX, BY), 0, s>>>(L, P.g.px, P.g.py, pj.z, pj.p[old],
+                                                                          pj.p[cur], pj.Ap, cg, rs);
 }
-void proj_update(const Params& P, const Projection& pj, int parity, CGScal* cg, const RedSlot& rs, int* iters_out,
-                 cudaGraphConditionalHandle cond, cudaStream_t s) {
+void proj_update_vcycle(const Params& P, const Projection& pj, int parity, CGScal* cg, const RedSlot& rs,
+                        const RedSlot& rs2, int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s) {
     const MGLevel& L = pj.lev[0];
     const int cur = parity & 1;
-    k_pcg_update<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, s>>>(L, pj.x, pj.r, pj.p[cur], pj.Ap, cg, rs, iters_out, cond);
-}
-void proj_vcycle(const Params& P, const Projection& pj, CGScal* cg, const RedSlot& rs, cudaStream_t s) {
-    vcycle(pj, 0, pj.r, pj.z, cg, rs, P.g.px, P.g.py, s);
+    if (pj.nlev == 1) {
+        k_pcg_update<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, s>>>(L, pj.x, pj.r[0], pj.p[cur], pj.Ap, cg, rs,
+                                                                iters_out, cond);
+        vcycle(pj, pj.r[0], nullptr, cg, rs, rs2, nullptr, 0, P.g.px, P.g.py, s);
+        return;
+    }
+    const CGFuse f{pj.r[cur], pj.Ap, pj.p[cur], pj.x, pj.r[cur ^ 1]};
+    vcycle(pj, pj.r[cur ^ 1], &f, cg, rs, rs2, iters_out, cond, P.g.px, P.g.py, s);
 }
 
 // ---- correction and diagnostics (Projection.jl:253-306) ---------------------------------------

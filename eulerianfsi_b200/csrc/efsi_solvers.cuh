@@ -13,16 +13,19 @@ struct CGScal {
 };
 
 // ---- viscous predictor (I - alpha*A) u = rhs with Dirichlet rows eliminated --------
+// Chronopoulos-Gear (single-reduction) Jacobi-PCG: one kernel per iteration.  r, w
+// (= A M r) and s (= A p) are ping-ponged between iterations (parity), so that the
+// neighbours read by one launch are never the values it writes.
 struct ViscSolve {
-    double *x_u, *x_v, *r_u, *r_v, *p_u[2], *p_v[2], *Ap_u, *Ap_v, *dinv_u, *dinv_v;
+    double *x_u, *x_v, *p_u, *p_v, *dinv_u, *dinv_v;
+    double *r_u[2], *r_v[2], *w_u[2], *w_v[2], *s_u[2], *s_v[2];
 };
 void visc_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const double* Un, const double* Vn,
                const double* rhs_u, const double* rhs_v, const double* phi, const ViscSolve& w, CGScal* cg,
+               const RedSlot& rs, const RedSlot& rs2, int* iters_out, cudaGraphConditionalHandle cond,
+               cudaStream_t s);
+void visc_iter(const Params& P, DtCoef alpha, const double* phi, const ViscSolve& w, int parity, CGScal* cg,
                const RedSlot& rs, int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s);
-void visc_matvec(const Params& P, DtCoef alpha, const double* phi, const ViscSolve& w, CGScal* cg, const RedSlot& rs,
-                 cudaStream_t s);
-void visc_update(const Params& P, const ViscSolve& w, CGScal* cg, const RedSlot& rs, int* iters_out,
-                 cudaGraphConditionalHandle cond, cudaStream_t s);
 void visc_enforce_dirichlet(const Params& P, const double* rhs_u, const double* rhs_v, double* x_u, double* x_v,
                             cudaStream_t s);
 
@@ -49,8 +52,9 @@ struct Projection {
     double* coarse_inv;   // dense inverse of the coarsest operator (shifted when singular)
     int nc;
     bool nullspace;
-    // fine-level CG vectors
-    double *x, *r, *z, *p[2], *Ap, *b, *rhs;
+    int nsm;              // multiprocessors (persistent launch grids)
+    // fine-level CG vectors (r ping-pongs between iterations when multigrid levels exist)
+    double *x, *r[2], *z, *p[2], *Ap, *b, *rhs;
     double *Up, *Vp;      // predictor velocity (full MAC arrays)
 };
 // Per-projection scalars: [0] defect, [1] scale, [2] sum b, [3] |rhs|^2, [4] wl2(div)^2,
@@ -65,13 +69,16 @@ void proj_cg_init(const Params& P, const Projection& pj, double reltol, int maxi
                   const ProjScal* ps, const RedSlot& rs, const RedSlot& rs2, const DevStatus* st, int* iters_out,
                   cudaGraphConditionalHandle cond, cudaStream_t s);
 void proj_matvec(const Params& P, const Projection& pj, int parity, CGScal* cg, const RedSlot& rs, cudaStream_t s);
-void proj_update(const Params& P, const Projection& pj, int parity, CGScal* cg, const RedSlot& rs, int* iters_out,
-                 cudaGraphConditionalHandle cond, cudaStream_t s);
-void proj_vcycle(const Params& P, const Projection& pj, CGScal* cg, const RedSlot& rs, cudaStream_t s);
+// CG update (x += a p, r -= a Kp, convergence) fused with the multigrid V-cycle z = M r.
+void proj_update_vcycle(const Params& P, const Projection& pj, int parity, CGScal* cg, const RedSlot& rs,
+                        const RedSlot& rs2, int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s);
 void proj_finish(const Params& P, const Projection& pj, const double* G, double* q_out, double* U_out,
                  double* V_out, ProjScal* ps, double* stage_linf, const RedSlot& rs1, const RedSlot& rs2,
                  DevStatus* st, cudaStream_t s);
-// Number of kernel launches of one projection CG iteration (statistics).
-int proj_kernels_per_iter(const Projection& pj);
+// Kernel launches of proj_update_vcycle and of proj_cg_init (statistics).
+int proj_update_vcycle_kernels(const Projection& pj);
+int proj_init_kernels(const Projection& pj);
+// Algorithmic bytes of one proj_update_vcycle (unique FP64 words read + written once).
+double proj_update_vcycle_bytes(const Projection& pj);
 
 }  // namespace efsi

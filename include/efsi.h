@@ -199,11 +199,11 @@ typedef struct efsi_projection_result {
 #define EFSI_SITE_MOMENTUM        1   /* explicit momentum forcing                       */
 #define EFSI_SITE_STRUCTURE       2   /* structure-tensor right-hand side                */
 #define EFSI_SITE_VISC_APPLY      3   /* viscous operator history I_uv                   */
-#define EFSI_SITE_VISC_MATVEC     4   /* viscous CG: p update + (I - a A) p + p.Ap        */
-#define EFSI_SITE_VISC_UPDATE     5   /* viscous CG: x, r update + norms                 */
+#define EFSI_SITE_VISC_CG         4   /* viscous CG: one single-reduction iteration      */
+#define EFSI_SITE_VISC_INIT       5   /* viscous CG: start vector, residual, A M r0      */
 #define EFSI_SITE_PCG_MATVEC      6   /* projection CG: p update + K p + p.Kp            */
-#define EFSI_SITE_PCG_UPDATE      7   /* projection CG: x, r update + |r|^2              */
-#define EFSI_SITE_VCYCLE          8   /* one multigrid V-cycle (all its kernels)         */
+#define EFSI_SITE_PCG_UPDATE      7   /* projection CG: x, r update + |r|^2 (no MG levels) */
+#define EFSI_SITE_VCYCLE          8   /* CG update fused with one multigrid V-cycle       */
 #define EFSI_SITE_PROJ_RHS        9   /* predictor injection + Poisson right-hand side   */
 #define EFSI_SITE_PROJ_FINISH    10   /* correction, velocity update, diagnostics        */
 #define EFSI_SITE_COMBINE        11   /* stage combination of phi, sigma, c              */
