@@ -239,13 +239,16 @@ __device__ __forceinline__ void visc_stage_value(const Params& P, const ViscIter
     if (!((inx || P.g.px) && (iny || P.g.py))) return;
     const size_t k = cidx(inx ? gi : wrapm(gi, Nx), iny ? gj : wrapm(gj, Ny), Nx);
     if (INIT) {
-        hu = v.dinv_u[k] * v.r_u[k];
-        hv = v.dinv_v[k] * v.r_v[k];
+        hu = __ldg(v.dinv_u + k) * __ldg(v.r_u + k);
+        hv = __ldg(v.dinv_v + k) * __ldg(v.r_v + k);
     } else {
-        double s1 = first ? v.w_u[k] : v.w_u[k] + b * v.s_u[k];
-        double s2 = first ? v.w_v[k] : v.w_v[k] + b * v.s_v[k];
-        hu = v.dinv_u[k] * (v.r_u[k] - a * s1);
-        hv = v.dinv_v[k] * (v.r_v[k] - a * s2);
+        const double d1 = __ldg(v.dinv_u + k), d2 = __ldg(v.dinv_v + k);
+        const double r1 = __ldg(v.r_u + k), r2 = __ldg(v.r_v + k);
+        const double w1 = __ldg(v.w_u + k), w2 = __ldg(v.w_v + k);
+        const double s1 = first ? w1 : w1 + b * __ldg(v.s_u + k);
+        const double s2 = first ? w2 : w2 + b * __ldg(v.s_v + k);
+        hu = d1 * (r1 - a * s1);
+        hv = d2 * (r2 - a * s2);
     }
 }
 
@@ -310,22 +313,41 @@ __global__ void __launch_bounds__(VTX * VTY, 4) k_visc_cg(Params P, DtCoef ac, c
         const int i0 = (t % ntx) * VTX, j0 = (t / ntx) * VTY;
         const int i = i0 + tx, j = j0 + ty;
         const bool own = i < Nx && j < Ny;
+        // every global load of the tile is issued before the first store
+        double d1 = 0.0, d2 = 0.0, r1 = 0.0, r2 = 0.0, w1 = 0.0, w2 = 0.0, s1 = 0.0, s2 = 0.0;
+        double p1 = 0.0, p2 = 0.0, x1 = 0.0, x2 = 0.0;
+        size_t k = 0;
+        if (own) {
+            k = cidx(i, j, Nx);
+            d1 = __ldg(v.dinv_u + k); d2 = __ldg(v.dinv_v + k);
+            r1 = __ldg(v.r_u + k); r2 = __ldg(v.r_v + k);
+            w1 = __ldg(v.w_u + k); w2 = __ldg(v.w_v + k);
+            if (!first) {
+                s1 = __ldg(v.s_u + k); s2 = __ldg(v.s_v + k);
+                p1 = v.p_u[k]; p2 = v.p_v[k];
+            }
+            x1 = v.x_u[k]; x2 = v.x_v[k];
+        }
+        const bool halo = tid < 2 * VSX + 2 * VTY;
+        int hx = 0, hy = 0;
+        double hu = 0.0, hv = 0.0;
+        if (halo) {
+            visc_halo_slot(tid, hx, hy);
+            visc_stage_value<false>(P, v, first, a, b, i0 + hx - 1, j0 + hy - 1, hu, hv);
+        }
         double un = 0.0, vn = 0.0;
         if (own) {
-            const size_t k = cidx(i, j, Nx);
-            const double d1 = v.dinv_u[k], d2 = v.dinv_v[k];
-            const double r1 = v.r_u[k], r2 = v.r_v[k];
-            const double s1 = first ? v.w_u[k] : v.w_u[k] + b * v.s_u[k];
-            const double s2 = first ? v.w_v[k] : v.w_v[k] + b * v.s_v[k];
-            const double p1 = first ? d1 * r1 : d1 * r1 + b * v.p_u[k];
-            const double p2 = first ? d2 * r2 : d2 * r2 + b * v.p_v[k];
+            s1 = first ? w1 : w1 + b * s1;
+            s2 = first ? w2 : w2 + b * s2;
+            p1 = first ? d1 * r1 : d1 * r1 + b * p1;
+            p2 = first ? d2 * r2 : d2 * r2 + b * p2;
+            const double q1 = r1 - a * s1, q2 = r2 - a * s2;
             v.p_u[k] = p1;
             v.p_v[k] = p2;
-            v.x_u[k] += a * p1;
-            v.x_v[k] += a * p2;
+            v.x_u[k] = x1 + a * p1;
+            v.x_v[k] = x2 + a * p2;
             v.sn_u[k] = s1;
             v.sn_v[k] = s2;
-            const double q1 = r1 - a * s1, q2 = r2 - a * s2;
             v.rn_u[k] = q1;
             v.rn_v[k] = q2;
             un = d1 * q1;
@@ -337,13 +359,9 @@ __global__ void __launch_bounds__(VTX * VTY, 4) k_visc_cg(Params P, DtCoef ac, c
         }
         su[(ty + 1) * VSX + tx + 1] = un;
         sv[(ty + 1) * VSX + tx + 1] = vn;
-        if (tid < 2 * VSX + 2 * VTY) {
-            int lx, ly;
-            visc_halo_slot(tid, lx, ly);
-            double hu, hv;
-            visc_stage_value<false>(P, v, first, a, b, i0 + lx - 1, j0 + ly - 1, hu, hv);
-            su[ly * VSX + lx] = hu;
-            sv[ly * VSX + lx] = hv;
+        if (halo) {
+            su[hy * VSX + hx] = hu;
+            sv[hy * VSX + hx] = hv;
         }
         __syncthreads();
         if (own) {
@@ -637,7 +655,7 @@ __device__ __forceinline__ double prolong(const MGLevel& C, int px, int py, cons
     int I0, I1, J0, J1;
     pair(i, C.nx, px, I0, I1);
     pair(j, C.ny, py, J0, J1);
-    auto E = [&](int a, int b) { return e[cidx(a, b, C.nx)]; };
+    auto E = [&](int a, int b) { return __ldg(e + cidx(a, b, C.nx)); };
     return 0.75 * (0.75 * E(I0, J0) + 0.25 * E(I1, J0)) + 0.25 * (0.75 * E(I0, J1) + 0.25 * E(I1, J1));
 }
 
@@ -704,7 +722,7 @@ struct CGFuse {
 // FUSE: b is r_new of the CG update, formed on the fly over the halo; the owned cells
 // of r_new and x are written and |r_new|^2 decides convergence.
 template <int T, bool FUSE>
-__global__ void __launch_bounds__(256, 6) k_mg_down(MGLevel L, MGLevel C, int px, int py,
+__global__ void __launch_bounds__(256, 4) k_mg_down(MGLevel L, MGLevel C, int px, int py,
                                                     const double* __restrict__ b, CGFuse f, CGScal* cg, RedSlot rs,
                                                     int* iters_out, cudaGraphConditionalHandle cond) {
     constexpr int H = 3, W = T + 2 * H;
@@ -723,42 +741,61 @@ __global__ void __launch_bounds__(256, 6) k_mg_down(MGLevel L, MGLevel C, int px
         const int bx = t % ntx, by = t / ntx;
         const int i0 = bx * T, j0 = by * T;
         const bool inner = inner_tile(L, i0, j0, T, H);
-        for (int s = tid; s < W * W; s += 256) {
-            const int lx = s % W, ly = s / W;
-            const int gi = i0 + lx - H, gj = j0 + ly - H;
-            double v = 0.0, d = 0.0;
-            size_t k = 0;
-            bool have = inner, own = false;
+        // load b (FUSE: r_old - a Kp) over the region; loads are batched per thread
+        constexpr int NS = (W * W + 255) / 256;
+        double vb[NS], vd[NS];
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            const int s = tid + q * 256;
+            vb[q] = 0.0;
+            vd[q] = 0.0;
+            if (s >= W * W) continue;
+            const int gi = i0 + s % W - H, gj = j0 + s / W - H;
+            size_t k;
             if (inner) {
                 k = cidx(gi, gj, nx);
-                d = d0;
-                own = lx >= H && lx < H + T && ly >= H && ly < H + T;
+                vd[q] = d0;
             } else {
-                const SlotPos q = slot_pos(L, px, py, gi, gj);
-                have = q.valid;
-                if (have) {
-                    k = cidx(q.wi, q.wj, nx);
-                    lev_diag(L, px, py, q.wi, q.wj, d);
-                    own = gi == q.wi && gj == q.wj && lx >= H && lx < H + T && ly >= H && ly < H + T;
-                }
+                const SlotPos sp = slot_pos(L, px, py, gi, gj);
+                if (!sp.valid) continue;
+                k = cidx(sp.wi, sp.wj, nx);
+                lev_diag(L, px, py, sp.wi, sp.wj, vd[q]);
             }
-            if (have) {
-                if (FUSE) {
-                    v = f.r_old[k] - a * f.Ap[k];
-                    if (own) {
-                        f.r_new[k] = v;
-                        f.x[k] += a * f.p[k];
-                        acc[0] += v * v;
-                    }
-                } else {
-                    v = b[k];
-                }
-            }
-            sb[s] = v;
-            sd[s] = d;
-            sx[s] = (have && ((lx + ly) & 1) == 0) ? v / d : 0.0;
+            vb[q] = FUSE ? __ldg(f.r_old + k) - a * __ldg(f.Ap + k) : __ldg(b + k);
+        }
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            const int s = tid + q * 256;
+            if (s >= W * W) continue;
+            const int lx = s % W, ly = s / W;
+            sb[s] = vb[q];
+            sd[s] = vd[q];
+            sx[s] = (vd[q] != 0.0 && ((lx + ly) & 1) == 0) ? vb[q] / vd[q] : 0.0;
         }
         __syncthreads();
+        if (FUSE) {  // owned cells: r_new, x += a p, |r_new|^2
+            constexpr int NO = T * T / 256;
+            double pv[NO], xv[NO];
+            size_t kk[NO];
+            bool in[NO];
+#pragma unroll
+            for (int q = 0; q < NO; ++q) {
+                const int s = tid + q * 256, lx = s % T, ly = s / T;
+                in[q] = i0 + lx < nx && j0 + ly < L.ny;
+                kk[q] = cidx(i0 + lx, j0 + ly, nx);
+                pv[q] = in[q] ? f.p[kk[q]] : 0.0;
+                xv[q] = in[q] ? f.x[kk[q]] : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < NO; ++q) {
+                if (!in[q]) continue;
+                const int s = tid + q * 256, lx = s % T, ly = s / T;
+                const double v = sb[(ly + H) * W + lx + H];
+                f.r_new[kk[q]] = v;
+                f.x[kk[q]] = xv[q] + a * pv[q];
+                acc[0] += v * v;
+            }
+        }
         // black cells within halo 2
         constexpr int B = T + 4;
         for (int s = tid; s < B * B / 2; s += 256) {
@@ -827,7 +864,7 @@ __global__ void __launch_bounds__(256, 6) k_mg_down(MGLevel L, MGLevel C, int px
 // Up leg of one level: x + P e (bilinear prolongation), then the post-smoothing
 // black-then-red Gauss-Seidel sweep; on the finest level also r.z for CG.
 template <int T, bool DOT>
-__global__ void __launch_bounds__(256, 6) k_mg_up(MGLevel L, MGLevel C, int px, int py,
+__global__ void __launch_bounds__(256, 4) k_mg_up(MGLevel L, MGLevel C, int px, int py,
                                                   const double* __restrict__ x, const double* __restrict__ e,
                                                   const double* __restrict__ b, double* xo, CGScal* cg, RedSlot rs) {
     constexpr int H = 2, W = T + 2 * H;
@@ -844,27 +881,36 @@ __global__ void __launch_bounds__(256, 6) k_mg_up(MGLevel L, MGLevel C, int px, 
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const int i0 = (t % ntx) * T, j0 = (t / ntx) * T;
         const bool inner = inner_tile(L, i0, j0, T, H);
-        for (int s = tid; s < W * W; s += 256) {
-            const int lx = s % W, ly = s / W;
-            const int gi = i0 + lx - H, gj = j0 + ly - H;
-            double xv = 0.0, bv = 0.0, d = 0.0;
+        constexpr int NS = (W * W + 255) / 256;
+        double xv[NS], bv[NS], dv[NS];
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            const int s = tid + q * 256;
+            xv[q] = 0.0;
+            bv[q] = 0.0;
+            dv[q] = 0.0;
+            if (s >= W * W) continue;
+            int wi = i0 + s % W - H, wj = j0 + s / W - H;
             if (inner) {
-                const size_t k = cidx(gi, gj, nx);
-                xv = x[k] + prolong(C, px, py, e, gi, gj);
-                bv = b[k];
-                d = d0;
+                dv[q] = d0;
             } else {
-                const SlotPos q = slot_pos(L, px, py, gi, gj);
-                if (q.valid) {
-                    const size_t k = cidx(q.wi, q.wj, nx);
-                    xv = x[k] + prolong(C, px, py, e, q.wi, q.wj);
-                    bv = b[k];
-                    lev_diag(L, px, py, q.wi, q.wj, d);
-                }
+                const SlotPos sp = slot_pos(L, px, py, wi, wj);
+                if (!sp.valid) continue;
+                wi = sp.wi;
+                wj = sp.wj;
+                lev_diag(L, px, py, wi, wj, dv[q]);
             }
-            sx[s] = xv;
-            sb[s] = bv;
-            sd[s] = d;
+            const size_t k = cidx(wi, wj, nx);
+            xv[q] = __ldg(x + k) + prolong(C, px, py, e, wi, wj);
+            bv[q] = __ldg(b + k);
+        }
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            const int s = tid + q * 256;
+            if (s >= W * W) continue;
+            sx[s] = xv[q];
+            sb[s] = bv[q];
+            sd[s] = dv[q];
         }
         __syncthreads();
         // black cells within halo 1
@@ -947,7 +993,7 @@ static void vcycle(const Projection& pj, const double* r_fine, const CGFuse* fus
     // 32x32 tiles while they fill the device, 16x16 below (shorter dependent chains)
     auto wide = [&](const MGLevel& L) { return ((L.nx + 31) / 32) * ((L.ny + 31) / 32) >= pj.nsm; };
     auto grid = [&](const MGLevel& L, int T) {
-        return persistent_grid(((L.nx + T - 1) / T) * ((L.ny + T - 1) / T), pj.nsm, 6);
+        return persistent_grid(((L.nx + T - 1) / T) * ((L.ny + T - 1) / T), pj.nsm, 4);
     };
     for (int l = 0; l + 1 < n; ++l) {
         const MGLevel &L = pj.lev[l], &C = pj.lev[l + 1];
