@@ -142,6 +142,9 @@ CUDA_ONLY = {
     "set_timed_site": (c_int32, [_H, c_int32]),
     "integrate_step_host": (c_int32, [_H] + [_dp] * 8 + [c_double, c_double, POINTER(StepReportC)]),
     "step_n": (c_int32, [_H, c_double, _dp, c_int32, POINTER(StepReportC)]),
+    # no handle: device pointers in, device result out (allocates nothing)
+    "divergence_residual_noalloc": (c_int32, [c_int32, c_int32, c_double, c_double, c_void_p, c_void_p,
+                                              c_void_p, c_void_p, c_void_p]),
 }
 
 PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))

@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1293,6 +1294,110 @@ int efsi_set_timed_site(efsi_handle* h, int32_t which) {
         h->stats.site_bytes = 0.0;
         h->site_used = 0;
         h->site_bytes_pending = 0.0;
+    });
+}
+
+}  // extern "C"
+
+// =========================================================================================
+// Allocation-free divergence residual (no counterpart in the reference)
+// =========================================================================================
+// Every other entry point works on a handle whose buffers efsi_create allocated.
+// Some callers cannot allow a library to call cudaMalloc: hosts that hand all device
+// memory out of their own pool allocator, and loops that must not meet the device-wide
+// synchronisation that cudaMalloc/cudaFree may imply.  This entry point computes the
+// stage-1 check of the IMEX step (max |div v - G|) on caller-owned device arrays with
+// its reduction scratch in a fixed static device array instead of allocated buffers.
+namespace {
+
+constexpr int kNoAllocBlockX = 32, kNoAllocBlockY = 8;
+// Block partials (two per block: max |div - G|, max |G|) and the completion ticket.
+// 16384 blocks of 32x8 cells cover up to 4,194,304 cells (2048 x 2048); 256 KiB that
+// every GPU which loads the library keeps until the process exits.
+constexpr int kNoAllocMaxBlocks = 16384;
+static __device__ __align__(256) double g_noalloc_scratch[2 * kNoAllocMaxBlocks + 32];
+
+// Device address of g_noalloc_scratch per device ordinal, looked up once per device.
+std::mutex g_noalloc_mutex;
+double* g_noalloc_base[256] = {};
+
+double* noalloc_scratch(int device) {
+    if (device < 0 || device >= 256) throw Err{EFSI_CUDA, "device ordinal out of range"};
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_base[device]) {
+        double* p = nullptr;
+        check_cuda(cudaGetSymbolAddress((void**)&p, g_noalloc_scratch), "scratch address");
+        g_noalloc_base[device] = p;
+    }
+    return g_noalloc_base[device];
+}
+
+void require_device_pointer(const void* p, int device, const char* name) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        throw Err{EFSI_ARG, std::string(name) + " is not a CUDA device pointer"};
+    }
+    if (!((a.type == cudaMemoryTypeDevice && a.device == device) || a.type == cudaMemoryTypeManaged))
+        throw Err{EFSI_ARG, std::string(name) + " must point to device (or managed) memory of the current device"};
+}
+
+// Same arithmetic as the stage-1 check of the step (k_stage1_check): per cell
+// |(U(i+1)-U(i))/hx + (V(j+1)-V(j))/hy - G| and |G|, max-reduced over the grid.
+__global__ void k_div_residual_noalloc(int Nx, int Ny, double ihx, double ihy, const double* __restrict__ U,
+                                       const double* __restrict__ V, const double* __restrict__ G, double* out,
+                                       RedSlot rs) {
+    __shared__ double sh[64];
+    const int i = blockIdx.x * kNoAllocBlockX + threadIdx.x, j = blockIdx.y * kNoAllocBlockY + threadIdx.y;
+    double v[2] = {0.0, 0.0};
+    if (i < Nx && j < Ny) {
+        double div = (U[uidx(i + 1, j, Nx)] - U[uidx(i, j, Nx)]) * ihx + (V[vidx(i, j + 1, Nx)] - V[vidx(i, j, Nx)]) * ihy;
+        double g = G ? G[cidx(i, j, Nx)] : 0.0;
+        v[0] = fabs(div - g);
+        v[1] = fabs(g);
+    }
+    double tot[2];
+    if (grid_reduce<2, true>(v, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0) {
+        out[0] = tot[0];
+        out[1] = tot[1];
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int efsi_divergence_residual_noalloc(int32_t Nx, int32_t Ny, double Lx, double Ly, const double* U, const double* V,
+                                     const double* G, double* out, void* stream) {
+    return guarded(nullptr, [&] {
+        if (Nx < 1 || Ny < 1) throw Err{EFSI_ARG, "Nx and Ny must be at least 1."};
+        if (!(std::isfinite(Lx) && Lx > 0.0 && std::isfinite(Ly) && Ly > 0.0))
+            throw Err{EFSI_ARG, "Lx and Ly must be finite and positive."};
+        const long long bx = (Nx + kNoAllocBlockX - 1) / kNoAllocBlockX, by = (Ny + kNoAllocBlockY - 1) / kNoAllocBlockY;
+        if (bx * by > kNoAllocMaxBlocks)
+            throw Err{EFSI_ARG, "efsi_divergence_residual_noalloc: a " + std::to_string(Nx) + " x " + std::to_string(Ny) +
+                                    " grid needs " + std::to_string(bx * by) + " reduction blocks of 32x8 cells; its "
+                                    "fixed scratch holds at most " + std::to_string(kNoAllocMaxBlocks) +
+                                    " (4,194,304 cells, e.g. 2048 x 2048)."};
+        if (!U || !V || !out) throw Err{EFSI_ARG, "U, V and out must not be NULL."};
+        int device = 0;
+        check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+        require_device_pointer(U, device, "U");
+        require_device_pointer(V, device, "V");
+        if (G) require_device_pointer(G, device, "G");
+        require_device_pointer(out, device, "out");
+        double* base = noalloc_scratch(device);
+        RedSlot rs;
+        rs.part = base;
+        rs.ticket = reinterpret_cast<unsigned*>(base + 2 * kNoAllocMaxBlocks);
+        rs.maxBlocks = kNoAllocMaxBlocks;
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        // The ticket must start at zero; partials are written before they are read.
+        check_cuda(cudaMemsetAsync(rs.ticket, 0, sizeof(unsigned), s), "scratch reset");
+        const double hx = Lx / Nx, hy = Ly / Ny;
+        k_div_residual_noalloc<<<dim3((unsigned)bx, (unsigned)by), dim3(kNoAllocBlockX, kNoAllocBlockY), 0, s>>>(
+            Nx, Ny, 1.0 / hx, 1.0 / hy, U, V, G, out, rs);
+        check_cuda(cudaGetLastError(), "launch");
     });
 }
 

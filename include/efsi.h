@@ -310,6 +310,32 @@ EFSI_API int efsi_get_stats(const efsi_handle* h, efsi_stats* stats);
  * efsi_stats.  Tracing aid of the benchmark; no reference counterpart. */
 EFSI_API int efsi_set_timed_site(efsi_handle* h, int32_t site);
 
+/* Allocation-free check of a MAC velocity against a divergence target: writes
+ * out[0] = max |div(U,V) - G| and out[1] = max |G| over the Nx x Ny cells of a
+ * uniform grid on [0,Lx] x [0,Ly] (G may be NULL for a zero target; the same
+ * quantity as the step's stage-1 check and ProjectionResult.constraint_linf).
+ * No counterpart in the reference: it exists for callers that cannot let a library
+ * allocate device memory, such as hosts that hand out all GPU memory from their own
+ * pool allocator, or loops that cannot absorb the device-wide synchronisation that
+ * cudaMalloc/cudaFree may cause.  It needs no handle, calls no allocator, and works
+ * directly on the caller's device arrays (U (Nx+1) x Ny, V Nx x (Ny+1), G and out
+ * on the current device).
+ *  - Asynchronous: the kernel runs on `stream` (a cudaStream_t; NULL is the legacy
+ *    default stream); out is valid once that stream has been synchronised.
+ *  - Scratch: a fixed 256 KiB static device array inside the library holds the
+ *    reduction partials, so the grid may hold at most 16384 blocks of 32 x 8 cells
+ *    (4,194,304 cells, e.g. 2048 x 2048); larger grids return EFSI_ARG.
+ *  - All calls on one device share that array: calls that may overlap on the GPU
+ *    (on different streams, or from different host threads) race and give wrong
+ *    results.  Serialise them.
+ *  - The first call on each device looks up the array's device address; make that
+ *    first call before beginning any stream capture.
+ * Errors return EFSI_ARG / EFSI_CUDA with the message in efsi_last_error(NULL)
+ * (per host thread). */
+EFSI_API int efsi_divergence_residual_noalloc(int32_t Nx, int32_t Ny, double Lx, double Ly,
+                                              const double* U, const double* V, const double* G,
+                                              double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
