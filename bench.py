@@ -34,6 +34,11 @@ sys.path.insert(0, ROOT)
 METRIC = "grid-cell-steps/s"
 UNIT = "cell-steps/s"
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from the ncu
+# capture summarised in the named profile; None where no capture exists.
+MEASURED_TRAFFIC = {
+    "visc_cg": (145.0e6, "profiles/k_visc_cg_cavity_disks20_N1024.md"),
+}
 
 
 def _peaks():
@@ -243,7 +248,9 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": args.site, "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": args.traffic,
+                     "frac": (achieved / peak) if achieved else None,
+                     "traffic": args.traffic if args.traffic is not None else
+                     (MEASURED_TRAFFIC[args.site][0] if args.site in MEASURED_TRAFFIC and args.N == 1024 else None),
                      "avg_launch_us": site_ms * 1e3, "algorithmic_bytes_per_launch": site_bytes,
                      "launches_timed": sst["site_launches"], "site_steps": site_steps},
         "clocks": clocks.summary(),
