@@ -91,6 +91,8 @@ struct efsi_handle {
     double *rhs_u, *rhs_v, *rhs_c;
     double *kappa, *cap_a, *cap_b;
     ViscSolve vs{};
+    ViscMixed vm{};     // precision form: FP32 vectors of the refined viscous solve
+    bool mixed = false;
     ScalarSolve ds{};
     Projection pj{};
     DevBlock* dev = nullptr;   // device scalars
@@ -739,6 +741,24 @@ void enqueue_step(efsi_handle* h) {
             if (h->visc) {
                 DtCoef alpha{dtp, c_AI_diag[st]};
                 const int maxit = std::max(1, P.nu.linear_maxiter);
+                if (h->mixed) {
+                    solve(
+                        h, KIND_VISC, st, &d->cg_visc, maxit, 2, 2,
+                        [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
+                            site(h, EFSI_SITE_VISC_INIT, 8.0 * N * 10.0, [&] {
+                                visc_mx_init(P, alpha, P.nu.linear_reltol, maxit, h->U, h->V, h->rhs_u, h->rhs_v,
+                                             h->phis, h->vs, h->vm, &d->cg_visc, h->slot[0], io, ch, ss);
+                            });
+                            h->launches += 2;
+                        },
+                        [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
+                            for (int k = 0; k < 2; ++k)  // FP32 vectors: 104 B per point per iteration
+                                site(h, EFSI_SITE_VISC_CG, 8.0 * N * 13.0, [&] {
+                                    visc_mx_iter(P, alpha, h->phis, h->rhs_u, h->rhs_v, h->vs, h->vm, k,
+                                                 &d->cg_visc, h->slot[2], io, ch, ss);
+                                });
+                        });
+                } else
                 solve(
                     h, KIND_VISC, st, &d->cg_visc, maxit, 2, 2,
                     [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
@@ -1016,6 +1036,19 @@ int efsi_create(const efsi_config* cfg, efsi_handle** out) {
             vs.r_u[k] = h->dalloc<double>(N); vs.r_v[k] = h->dalloc<double>(N);
             vs.w_u[k] = h->dalloc<double>(N); vs.w_v[k] = h->dalloc<double>(N);
             vs.s_u[k] = h->dalloc<double>(N); vs.s_v[k] = h->dalloc<double>(N);
+        }
+        h->mixed = P.nu.precision == EFSI_PRECISION_MIXED;
+        if (P.nu.precision != EFSI_PRECISION_FP64 && !h->mixed) throw Err{EFSI_ARG, "unknown precision form"};
+        if (h->mixed && h->visc) {
+            ViscMixed& m = h->vm;
+            for (int k = 0; k < 2; ++k) {
+                m.r_u[k] = h->dalloc<float>(N); m.r_v[k] = h->dalloc<float>(N);
+                m.w_u[k] = h->dalloc<float>(N); m.w_v[k] = h->dalloc<float>(N);
+                m.s_u[k] = h->dalloc<float>(N); m.s_v[k] = h->dalloc<float>(N);
+            }
+            m.p_u = h->dalloc<float>(N); m.p_v = h->dalloc<float>(N);
+            m.dinv_u = h->dalloc<float>(N); m.dinv_v = h->dalloc<float>(N);
+            m.rR_u = h->dalloc<float>(N); m.rR_v = h->dalloc<float>(N);
         }
         ScalarSolve& ds = h->ds;
         ds.x = h->cs; ds.r = h->dalloc<double>(N);

@@ -425,6 +425,219 @@ void visc_iter(const Params& P, DtCoef alpha, const double* phi, const ViscSolve
                                                                         iters_out, cond);
 }
 
+// ---- precision form of the viscous solve -------------------------------------------------
+enum { MX_ITER = 0, MX_REFINE = 1, MX_RESTART = 2 };
+// The FP32 recurrence runs until its residual has dropped by this factor (squared:
+// 1e-4 in norm) below the residual of its restart, or below the solve's target.
+constexpr double kMxInnerDrop2 = 1e-8;
+
+struct ViscMxArgs {
+    const float *r_u, *r_v, *w_u, *w_v, *s_u, *s_v;  // iteration i (read)
+    float *rn_u, *rn_v, *wn_u, *wn_v, *sn_u, *sn_v;  // iteration i+1 (written)
+    float *p_u, *p_v, *dinv_u, *dinv_v, *rR_u, *rR_v;
+    double *x_u, *x_v;
+    const double *rhs_u, *rhs_v;
+};
+
+// FP64 value staged at tile slot (gi, gj): x (REFINE/START), M rR (RESTART) or
+// M (r_i - a (w_i + b s_{i-1})) (ITER); zero outside walls, wrapped when periodic.
+__device__ __forceinline__ void visc_mx_slot(const Params& P, const ViscMxArgs& v, int phase, bool first, double a,
+                                             double b, int gi, int gj, double& hu, double& hv) {
+    const int Nx = P.g.Nx, Ny = P.g.Ny;
+    const bool inx = gi >= 0 && gi < Nx, iny = gj >= 0 && gj < Ny;
+    hu = 0.0;
+    hv = 0.0;
+    if (!((inx || P.g.px) && (iny || P.g.py))) return;
+    const size_t k = cidx(inx ? gi : wrapm(gi, Nx), iny ? gj : wrapm(gj, Ny), Nx);
+    if (phase == MX_REFINE) {
+        hu = v.x_u[k];
+        hv = v.x_v[k];
+    } else if (phase == MX_RESTART) {
+        hu = (double)v.dinv_u[k] * (double)v.rR_u[k];
+        hv = (double)v.dinv_v[k] * (double)v.rR_v[k];
+    } else {
+        const double w1 = __ldg(v.w_u + k), w2 = __ldg(v.w_v + k);
+        const double s1 = first ? w1 : w1 + b * (double)__ldg(v.s_u + k);
+        const double s2 = first ? w2 : w2 + b * (double)__ldg(v.s_v + k);
+        hu = (double)__ldg(v.dinv_u + k) * ((double)__ldg(v.r_u + k) - a * s1);
+        hv = (double)__ldg(v.dinv_v + k) * ((double)__ldg(v.r_v + k) - a * s2);
+    }
+}
+
+// One launch of the refined solve.  START: first launch of a solve (x = x0 given):
+// Jacobi diagonal, FP64 residual, tolerance.  Otherwise the phase stored in `cg`:
+//   ITER     one FP32 Chronopoulos-Gear iteration (x accumulates in FP64)
+//   REFINE   r = rhs - (I - alpha A) x in FP64; stop, or restart from it
+//   RESTART  w = A M r, r.Mr, Mr.w, from the refined residual
+template <bool START>
+__global__ void __launch_bounds__(VTX * VTY, 3) k_visc_mx(Params P, DtCoef ac, double reltol, int maxiter,
+                                                          const double* __restrict__ phi, ViscMxArgs v, CGScal* cg,
+                                                          RedSlot rs, int* iters_out,
+                                                          cudaGraphConditionalHandle cond) {
+    __shared__ double su[VSX * VSY], sv[VSX * VSY];
+    __shared__ double sh[3 * 32];
+    if (!START && cg->done) return;
+    const int phase = START ? MX_REFINE : cg->phase;
+    const double alpha = ac.value();
+    const bool first = START ? true : cg->inner == 0;
+    const double a = START ? 0.0 : cg->alpha, b = first ? 0.0 : cg->beta;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + ty * VTX;
+    const int Nx = P.g.Nx, Ny = P.g.Ny;
+    const int ntx = (Nx + VTX - 1) / VTX, nt = ntx * ((Ny + VTY - 1) / VTY);
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int i0 = (t % ntx) * VTX, j0 = (t / ntx) * VTY;
+        const int i = i0 + tx, j = j0 + ty;
+        const bool own = i < Nx && j < Ny;
+        const size_t k = own ? cidx(i, j, Nx) : 0;
+        double un = 0.0, vn = 0.0;
+        if (own && phase == MX_ITER) {
+            const double d1 = v.dinv_u[k], d2 = v.dinv_v[k];
+            const double r1 = v.r_u[k], r2 = v.r_v[k];
+            const double w1 = v.w_u[k], w2 = v.w_v[k];
+            double s1 = 0.0, s2 = 0.0, p1 = 0.0, p2 = 0.0;
+            if (!first) { s1 = v.s_u[k]; s2 = v.s_v[k]; p1 = v.p_u[k]; p2 = v.p_v[k]; }
+            const double x1 = v.x_u[k], x2 = v.x_v[k];
+            s1 = first ? w1 : w1 + b * s1;
+            s2 = first ? w2 : w2 + b * s2;
+            p1 = first ? d1 * r1 : d1 * r1 + b * p1;
+            p2 = first ? d2 * r2 : d2 * r2 + b * p2;
+            const double q1 = r1 - a * s1, q2 = r2 - a * s2;
+            v.p_u[k] = (float)p1;
+            v.p_v[k] = (float)p2;
+            v.x_u[k] = x1 + a * p1;
+            v.x_v[k] = x2 + a * p2;
+            v.sn_u[k] = (float)s1;
+            v.sn_v[k] = (float)s2;
+            v.rn_u[k] = (float)q1;
+            v.rn_v[k] = (float)q2;
+            un = d1 * q1;
+            vn = d2 * q2;
+            acc[0] += q1 * un + q2 * vn;
+            acc[2] += q1 * q1 + q2 * q2;
+        } else {
+            visc_mx_slot(P, v, phase, first, a, b, i, j, un, vn);
+        }
+        su[(ty + 1) * VSX + tx + 1] = un;
+        sv[(ty + 1) * VSX + tx + 1] = vn;
+        if (tid < 2 * VSX + 2 * VTY) {
+            int lx, ly;
+            visc_halo_slot(tid, lx, ly);
+            double hu, hv;
+            visc_mx_slot(P, v, phase, first, a, b, i0 + lx - 1, j0 + ly - 1, hu, hv);
+            su[ly * VSX + lx] = hu;
+            sv[ly * VSX + lx] = hv;
+        }
+        __syncthreads();
+        if (own) {
+            TileUV tl{su, sv, i0, j0, Nx, Ny};
+            MuField mu = make_mu(P, phi);
+            double au, av;
+            visc_A_any(P, mu, tl, i, j, au, av);
+            if (phase == MX_REFINE) {
+                if (START) {
+                    double du, dv;
+                    visc_diag(P, mu, i, j, du, dv);
+                    v.dinv_u[k] = u_fixed(P, i) ? 0.0f : (float)(1.0 / (1.0 - alpha * du));
+                    v.dinv_v[k] = v_fixed(P, j) ? 0.0f : (float)(1.0 / (1.0 - alpha * dv));
+                }
+                const double r1 = u_fixed(P, i) ? 0.0 : v.rhs_u[k] - (un - alpha * au);
+                const double r2 = v_fixed(P, j) ? 0.0 : v.rhs_v[k] - (vn - alpha * av);
+                v.rR_u[k] = (float)r1;
+                v.rR_v[k] = (float)r2;
+                acc[0] += r1 * r1 + r2 * r2;
+            } else {
+                const double w1 = u_fixed(P, i) ? 0.0 : un - alpha * au;
+                const double w2 = v_fixed(P, j) ? 0.0 : vn - alpha * av;
+                v.wn_u[k] = (float)w1;
+                v.wn_v[k] = (float)w2;
+                acc[1] += un * w1 + vn * w2;
+                if (phase == MX_RESTART) {
+                    const double r1 = v.rR_u[k], r2 = v.rR_v[k];
+                    v.rn_u[k] = (float)r1;
+                    v.rn_v[k] = (float)r2;
+                    acc[0] += r1 * un + r2 * vn;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    double tot[3];
+    if (grid_reduce<3>(acc, rs, tot, sh) && tid == 0) {
+        if (START) {
+            cg->rr0 = tot[0];
+            cg->rr = tot[0];
+            cg->tol2 = reltol * reltol * tot[0];
+            cg->iter = 0;
+            cg->maxiter = maxiter;
+            cg->alpha = 0.0;
+            cg->beta = 0.0;
+            cg->inner = 0;
+            cg->rr_restart = tot[0];
+            cg->conv = tot[0] == 0.0 ? 1 : 0;
+            cg->done = (cg->conv || !isfinite(tot[0])) ? 1 : 0;
+            cg->phase = MX_RESTART;
+            if (iters_out) *iters_out = 0;
+            set_loop(cond, !cg->done);
+            return;
+        }
+        cg->iter += 1;
+        if (phase == MX_ITER) {
+            const double g = tot[0], d = tot[1];
+            const double bn = cg->rz != 0.0 ? g / cg->rz : 0.0;
+            const double den = d - (cg->alpha != 0.0 ? bn * g / cg->alpha : 0.0);
+            cg->beta = bn;
+            cg->alpha = den != 0.0 ? g / den : 0.0;
+            cg->rz = g;
+            cg->pAp = d;
+            cg->inner += 1;
+            if (!isfinite(tot[2])) cg->done = 1;
+            else if (tot[2] <= cg->tol2 || tot[2] <= kMxInnerDrop2 * cg->rr_restart) cg->phase = MX_REFINE;
+        } else if (phase == MX_REFINE) {
+            cg->rr = tot[0];
+            if (tot[0] <= cg->tol2) { cg->conv = 1; cg->done = 1; }
+            else if (!isfinite(tot[0])) cg->done = 1;
+            else { cg->phase = MX_RESTART; cg->rr_restart = tot[0]; }
+        } else {  // restart: r.Mr and Mr.w of the refined residual
+            cg->rz = tot[0];
+            cg->pAp = tot[1];
+            cg->alpha = tot[1] != 0.0 ? tot[0] / tot[1] : 0.0;
+            cg->beta = 0.0;
+            cg->inner = 0;
+            cg->phase = MX_ITER;
+        }
+        if (!cg->done && cg->iter >= cg->maxiter) cg->done = 1;
+        if (iters_out) *iters_out = cg->iter;
+        set_loop(cond, !cg->done);
+    }
+}
+
+static ViscMxArgs visc_mx_args(const ViscSolve& w, const ViscMixed& m, const double* rhs_u, const double* rhs_v,
+                               int parity) {
+    const int c = parity & 1, n = c ^ 1;
+    return ViscMxArgs{m.r_u[c], m.r_v[c], m.w_u[c], m.w_v[c], m.s_u[c], m.s_v[c],
+                      m.r_u[n], m.r_v[n], m.w_u[n], m.w_v[n], m.s_u[n], m.s_v[n],
+                      m.p_u, m.p_v, m.dinv_u, m.dinv_v, m.rR_u, m.rR_v, w.x_u, w.x_v, rhs_u, rhs_v};
+}
+
+void visc_mx_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const double* Un, const double* Vn,
+                  const double* rhs_u, const double* rhs_v, const double* phi, const ViscSolve& w,
+                  const ViscMixed& m, CGScal* cg, const RedSlot& rs, int* iters_out,
+                  cudaGraphConditionalHandle cond, cudaStream_t s) {
+    k_visc_x0<<<grid2(P.g.Nx, P.g.Ny), dim3(BX, BY), 0, s>>>(P, Un, Vn, w.x_u, w.x_v);
+    const int nt = ((P.g.Nx + VTX - 1) / VTX) * ((P.g.Ny + VTY - 1) / VTY);
+    k_visc_mx<true><<<persistent_grid(nt, P.nsm, 3), dim3(VTX, VTY), 0, s>>>(
+        P, alpha, reltol, maxiter, phi, visc_mx_args(w, m, rhs_u, rhs_v, 0), cg, rs, iters_out, cond);
+}
+
+void visc_mx_iter(const Params& P, DtCoef alpha, const double* phi, const double* rhs_u, const double* rhs_v,
+                  const ViscSolve& w, const ViscMixed& m, int parity, CGScal* cg, const RedSlot& rs,
+                  int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s) {
+    const int nt = ((P.g.Nx + VTX - 1) / VTX) * ((P.g.Ny + VTY - 1) / VTY);
+    k_visc_mx<false><<<persistent_grid(nt, P.nsm, 3), dim3(VTX, VTY), 0, s>>>(
+        P, alpha, 0.0, 0, phi, visc_mx_args(w, m, rhs_u, rhs_v, parity), cg, rs, iters_out, cond);
+}
+
 // NoViscosity: predictor = rhs with the Dirichlet rows enforced (:786-788).
 __global__ void k_visc_enforce(Params P, const double* __restrict__ ru, const double* __restrict__ rv, double* xu,
                                double* xv) {

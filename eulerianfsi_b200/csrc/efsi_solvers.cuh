@@ -10,6 +10,10 @@ namespace efsi {
 struct CGScal {
     double rz, pAp, alpha, beta, rr, rr0, tol2;
     int iter, done, maxiter, conv;
+    // precision form: phase of the refined solve, inner iterations since the last
+    // restart, squared residual at that restart
+    int phase, inner;
+    double rr_restart;
 };
 
 // ---- viscous predictor (I - alpha*A) u = rhs with Dirichlet rows eliminated --------
@@ -26,6 +30,22 @@ void visc_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const 
                cudaStream_t s);
 void visc_iter(const Params& P, DtCoef alpha, const double* phi, const ViscSolve& w, int parity, CGScal* cg,
                const RedSlot& rs, int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s);
+// Precision form (EFSI_PRECISION_MIXED): the same Chronopoulos-Gear CG with FP32
+// vectors and FP64 x, inner products and scalars; when the FP32 recurrence has reduced
+// the residual by 1e-4, the true residual is recomputed in FP64 from x (iterative
+// refinement) and the recurrence restarts from it.  Both calls launch the same kernel;
+// device-side phases (iterate, refine, restart) decide what each launch does.
+struct ViscMixed {
+    float *r_u[2], *r_v[2], *w_u[2], *w_v[2], *s_u[2], *s_v[2];
+    float *p_u, *p_v, *dinv_u, *dinv_v, *rR_u, *rR_v;
+};
+void visc_mx_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const double* Un, const double* Vn,
+                  const double* rhs_u, const double* rhs_v, const double* phi, const ViscSolve& w,
+                  const ViscMixed& m, CGScal* cg, const RedSlot& rs, int* iters_out,
+                  cudaGraphConditionalHandle cond, cudaStream_t s);
+void visc_mx_iter(const Params& P, DtCoef alpha, const double* phi, const double* rhs_u, const double* rhs_v,
+                  const ViscSolve& w, const ViscMixed& m, int parity, CGScal* cg, const RedSlot& rs,
+                  int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s);
 void visc_enforce_dirichlet(const Params& P, const double* rhs_u, const double* rhs_v, double* x_u, double* x_v,
                             cudaStream_t s);
 

@@ -402,3 +402,32 @@ def test_step_n_matches_single_steps_and_reports_failing_step():
     after = st3.copy()
     gpu.download(after)
     np.testing.assert_array_equal(after.U, st3.U)
+
+
+def _steps_device(w, steps, compatible=False):
+    gpu, _ = pair(w.metrics, w.bcs, w.models, w.numerics)
+    st = w.state.copy()
+    gpu.upload(st)
+    gpu.set_correction(fz(w.metrics.Nx, w.metrics.Ny))
+    if compatible:
+        gpu.call("make_velocity_compatible", C.byref(_abi.ProjectionResultC()))
+    dts = (C.c_double * steps)(*([w.dt] * steps))
+    gpu.call("step_n", 0.0, dts, steps, None)
+    gpu.download(st)
+    return st, gpu.stats()
+
+
+@pytest.mark.parametrize("name", ["cavity_disk", "filament", "channel_growth"])
+def test_mixed_precision_step_close_to_fp64(name):
+    """Precision form: FP32 solver bulk with FP64 refinement stays within 1e-6
+    relative L2 of the FP64 step (both solved to the same tolerances)."""
+    make = {"cavity_disk": lambda p: workloads.cavity_disk(N=64, precision=p),
+            "filament": lambda p: workloads.filament_kolmogorov(N=64, precision=p),
+            "channel_growth": lambda p: workloads.channel_growth(N=32, precision=p)}[name]
+    comp = name == "channel_growth"
+    a, sa = _steps_device(make("fp64"), 10, comp)
+    b, sb = _steps_device(make("mixed"), 10, comp)
+    for f in ("U", "V", "phi", "resource", "sigma_xx", "sigma_yy", "sigma_xy"):
+        e = rel_err(getattr(b, f), getattr(a, f))
+        assert e <= 1e-6, (f, e)
+    assert sum(sb["velocity_iterations"]) > 0
