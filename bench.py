@@ -2,12 +2,15 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload: the 20-disk lid-driven cavity at 1024x1024 (ACDI, FP64, dt = 0.2 h), seeded
-synthetic initial fields.  A step is one integrate_step! of that grid.  `value` is
-timed with CUDA events on the library's stream around K device-resident steps
-(inputs already in HBM); `e2e` repeats the measurement through the public API
-(integrate_step with pinned host arrays, host<->device copies inside the timed
-region).  The working set (~0.5 GB) exceeds the 126 MB L2 on every step, so no
+Workload: the 20-disk lid-driven cavity at 1024x1024 (ACDI, dt = 0.2 h), seeded
+synthetic initial fields.  A step is one integrate_step! of that grid.  The headline
+is the precision form (FP32 solver bulk, FP64 state, residuals, inner products and
+refinement); the FP64 step is timed beside it from the same initial state and the
+per-field relative L2 difference of the two after W+K steps is reported
+(`vs_other_precision`).  `value` is timed with CUDA events on the library's stream
+around K device-resident steps (inputs already in HBM); `e2e` repeats the
+measurement through the public API (integrate_step with pinned host arrays,
+host<->device copies inside the timed region).  The working set (~0.5 GB) exceeds the 126 MB L2 on every step, so no
 extra L2 flush is inserted.  Multi-GPU runs are independent replicas (the step is a
 global elliptic solve and does not shard); rank 0 prints the aggregate.
 
@@ -37,7 +40,8 @@ FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from the ncu
 # capture summarised in the named profile; None where no capture exists.
 MEASURED_TRAFFIC = {
-    "visc_cg": (145.0e6, "profiles/k_visc_cg_cavity_disks20_N1024.md"),
+    ("visc_cg", "fp64"): (145.0e6, "profiles/k_visc_cg_cavity_disks20_N1024.md"),
+    ("visc_cg", "mixed"): (66.8e6, "profiles/k_visc_mx_cavity_disks20_N1024_mixed.md"),
 }
 
 
@@ -167,34 +171,62 @@ def run_ours(args, rank, world, local_rank):
     dist = None
     if world > 1:
         import torch.distributed as dist
-    w = build_workload(args, args.precision)
-    ctx = ef.build_imex_context(w.metrics, w.bcs, w.models, numerics=w.numerics)
-    h = ctx.handle
-    h.upload(w.state)
-    h.set_correction(np.zeros((args.N, args.N), order="F"))
-    dts = (C.c_double * max(args.warmup, args.steps, 1))(*([w.dt] * max(args.warmup, args.steps, 1)))
-    t = 0.0
-    if args.warmup:
-        h.call("step_n", t, dts, int(args.warmup), None)
-        t += args.warmup * w.dt
-    h.call("set_timed_site", -1)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local_rank) as clocks:
+    nd = max(args.warmup, args.steps, 1)
+
+    def timed(precision, sample_clocks):
+        """W untimed then K timed device-resident steps of one precision form."""
+        w = build_workload(args, precision)
+        ctx = ef.build_imex_context(w.metrics, w.bcs, w.models, numerics=w.numerics)
+        h = ctx.handle
+        h.upload(w.state)
+        h.set_correction(np.zeros((args.N, args.N), order="F"))
+        dts = (C.c_double * nd)(*([w.dt] * nd))
+        t = 0.0
+        if args.warmup:
+            h.call("step_n", t, dts, int(args.warmup), None)
+            t += args.warmup * w.dt
+        h.call("set_timed_site", -1)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local_rank) if sample_clocks else None
+        if clocks:
+            clocks.__enter__()
         h.call("step_n", t, dts, int(args.steps), None)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    t += args.steps * w.dt
-    st = h.stats()
-    ms = st["device_ms"]
+        torch.cuda.synchronize()
+        if clocks:
+            clocks.__exit__(None, None, None)
+        if dist:
+            dist.barrier()
+        st = h.stats()
+        ms = st["device_ms"]
+        if dist:
+            tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+        return dict(w=w, ctx=ctx, h=h, dts=dts, t=t + args.steps * w.dt, ms=ms, st=st, clocks=clocks)
+
+    other = "fp64" if args.precision == "mixed" else "mixed"
+    ref = None if args.no_compare else timed(other, False)
+    run = timed(args.precision, True)
+    w, ctx, h, dts, t, ms, st, clocks = (run[k] for k in ("w", "ctx", "h", "dts", "t", "ms", "st", "clocks"))
     launches = st["kernel_launches"]
-    if dist:
-        tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
     value = world * w.cells * args.steps / (ms / 1e3)
+    compare = None
+    if ref is not None:
+        sa, sb = w.state.copy(), ref["w"].state.copy()
+        h.download(sa)
+        ref["h"].download(sb)
+        errs = {}
+        for name in ("U", "V", "phi", "sigma_xx", "sigma_yy", "sigma_xy"):
+            a, b = getattr(sa, name), getattr(sb, name)
+            errs[name] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+        ref_value = world * w.cells * args.steps / (ref["ms"] / 1e3)
+        compare = {"precision": other, "value": ref_value, "ms_per_step": ref["ms"] / args.steps,
+                   "speedup": (value / ref_value) if args.precision == "mixed" else (ref_value / value),
+                   "rel_l2_after_steps": args.warmup + args.steps, "rel_l2": errs,
+                   "max_rel_l2": max(errs.values())}
+        ref["ctx"].handle.close()
 
     # ---- roofline of one kernel: the same steps enqueued from the host with CUDA events
     # around every launch of the site (per-launch events cannot sit inside graph loops)
@@ -241,7 +273,7 @@ def run_ours(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f64-state/f32-bulk", "data": "synthetic",
+        "dtype": "f64" if args.precision == "fp64" else "f32-solver-bulk/f64-state-refinement", "data": "synthetic",
         "config": config_block(args, args.precision),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps},
@@ -250,10 +282,12 @@ def run_ours(args, rank, world, local_rank):
                      "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
                      "traffic": args.traffic if args.traffic is not None else
-                     (MEASURED_TRAFFIC[args.site][0] if args.site in MEASURED_TRAFFIC and args.N == 1024 else None),
+                     (MEASURED_TRAFFIC[(args.site, args.precision)][0]
+                      if (args.site, args.precision) in MEASURED_TRAFFIC and args.N == 1024 else None),
                      "avg_launch_us": site_ms * 1e3, "algorithmic_bytes_per_launch": site_bytes,
                      "launches_timed": sst["site_launches"], "site_steps": site_steps},
         "clocks": clocks.summary(),
+        "vs_other_precision": compare,
         "solver": {"projection_iterations": st["projection_iterations"],
                    "velocity_iterations": st["velocity_iterations"]},
     }
@@ -272,7 +306,9 @@ def main():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--N", type=int, default=1024)
-    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    p.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
+                   help="headline precision form; the other form is timed beside it")
+    p.add_argument("--no-compare", action="store_true", help="skip the other precision form")
     p.add_argument("--projection-reltol", type=float, default=1e-10)
     p.add_argument("--velocity-reltol", type=float, default=1e-8)
     p.add_argument("--site", default="visc_cg")
