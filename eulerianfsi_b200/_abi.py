@@ -137,6 +137,7 @@ SIGNATURES = {
     "momentum_explicit_rhs": (c_int32, [_H, c_double] + [_dp] * 9),
     "apply_viscous_operator": (c_int32, [_H, _dp, _dp, _dp]),
     "get_stats": (c_int32, [_H, POINTER(Stats)]),
+    "uwcdi_strang_step": (c_int32, [_H, _dp, _dp, _dp, c_double, c_int32, _dp]),
 }
 CUDA_ONLY = {
     "set_timed_site": (c_int32, [_H, c_int32]),

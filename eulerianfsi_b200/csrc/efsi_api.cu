@@ -1255,6 +1255,32 @@ int efsi_phase_field_rhs(efsi_handle* h, const double* U, const double* V, const
     });
 }
 
+int efsi_uwcdi_strang_step(efsi_handle* h, const double* U, const double* V, const double* phi, double dt,
+                           int32_t x_first, double* out) {
+    return guarded(h, [&] {
+        if (h->P.md.phase_field_method != EFSI_PF_UWCDI) throw Err{EFSI_ARG, "context method is not UWCDI"};
+        if (!U || !V || !phi || !out) throw Err{EFSI_ARG, "U, V, phi and out must not be NULL"};
+        if (!std::isfinite(dt)) throw Err{EFSI_ARG, "dt must be finite."};
+        DevBlock* d = h->dev;
+        k_reset_call<<<1, 1, 0, h->stream>>>(d);
+        h2d(h, h->Us, U, h->nu); h2d(h, h->Vs, V, h->nv); h2d(h, h->phis, phi, h->nc);
+        // half sweep, full sweep in the other direction, half sweep (PhaseFieldMethods.jl:810-850)
+        const int a1 = x_first ? 1 : 2, a2 = 3 - a1;
+        const int axis[3] = {a1, a2, a1};
+        const double step[3] = {0.5 * dt, dt, 0.5 * dt};
+        const double* q = h->phis;
+        for (int k = 0; k < 3; ++k) {
+            if (step[k] == 0.0) continue;
+            launch_strang_sweep(h->P, h->Us, h->Vs, q, h->Ephi[k], axis[k], step[k], &d->st, h->stream);
+            q = h->Ephi[k];
+        }
+        fetch_dev(h);
+        raise_if_failed(h);
+        d2h(h, out, q, h->nc);
+        check_cuda(cudaStreamSynchronize(h->stream), "uwcdi_strang_step");
+    });
+}
+
 int efsi_structure_tensor_rhs(efsi_handle* h, const double* sxx, const double* syy, const double* sxy,
                               const double* U, const double* V, const double* phi, const double* G, double* rxx,
                               double* ryy, double* rxy) {

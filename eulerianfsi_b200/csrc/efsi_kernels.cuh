@@ -45,6 +45,9 @@ void launch_finalize(const Params& P, const double* Us, const double* Vs, const 
                      const DevStatus* st, cudaStream_t s);
 void launch_phase_rhs(const Params& P, const StageFields& f, const double* gamma_eff, double* Ephi,
                       DevStatus* st, cudaStream_t s);
+// One directional sweep of uwcdi_strang_step (axis 1 = x, 2 = y), out = phi - h div(F).
+void launch_strang_sweep(const Params& P, const double* U, const double* V, const double* phi, double* out, int axis,
+                         double h, DevStatus* st, cudaStream_t s);
 void launch_umax(const Params& P, const double* U, const double* V, double* out, const RedSlot& rs,
                  cudaStream_t s);
 void launch_copy(double* dst, const double* src, size_t n, cudaStream_t s);

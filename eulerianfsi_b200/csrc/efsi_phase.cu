@@ -29,11 +29,14 @@ __device__ __forceinline__ double pbv(const SideD& s, int k, double interior) {
     return interior;
 }
 
-template <int METHOD>
+// AXIS = 0: the phase-field right-hand side.  AXIS = 1 / 2: one directional sweep of
+// uwcdi_strang_step (PhaseFieldMethods.jl:810-850): out = phi - h div_x(F) (or div_y),
+// the flux of the other direction set to zero and no source term.
+template <int METHOD, int AXIS = 0>
 __global__ void __launch_bounds__(TX* TY) k_phase(Params P, const double* __restrict__ U, const double* __restrict__ V,
                                                   const double* __restrict__ phi, const double* __restrict__ G,
                                                   const double* __restrict__ gamma_dyn, double* out,
-                                                  DevStatus* st) {
+                                                  DevStatus* st, double h = 0.0) {
     __shared__ double s_phi[SY][SX];
     __shared__ double s_aux[SY][SX];
     __shared__ double s_nx[NY][NX];
@@ -256,6 +259,11 @@ __global__ void __launch_bounds__(TX* TY) k_phase(Params P, const double* __rest
             reg[dir][side] = rflux;
         }
     }
+    if (AXIS != 0) {
+        const double d = AXIS == 1 ? (conv[0][1] - conv[0][0]) * ihx : (conv[1][1] - conv[1][0]) * ihy;
+        out[cidx(i, j, Nx)] = pc + h * (-d);
+        return;
+    }
     double divc = (conv[0][1] - conv[0][0]) * ihx + (conv[1][1] - conv[1][0]) * ihy;
     double divr = (reg[0][1] - reg[0][0]) * ihx + (reg[1][1] - reg[1][0]) * ihy;
     double r;
@@ -282,6 +290,15 @@ void launch_phase_rhs(const Params& P, const StageFields& f, const double* gamma
             k_phase<EFSI_PF_UPWIND><<<grid, block, 0, s>>>(P, f.U, f.V, f.phi, f.G, gamma_eff, Ephi, st);
             break;
     }
+}
+
+void launch_strang_sweep(const Params& P, const double* U, const double* V, const double* phi, double* out, int axis,
+                         double h, DevStatus* st, cudaStream_t s) {
+    dim3 grid((P.g.Nx + TX - 1) / TX, (P.g.Ny + TY - 1) / TY), block(TX, TY);
+    if (axis == 1)
+        k_phase<EFSI_PF_UWCDI, 1><<<grid, block, 0, s>>>(P, U, V, phi, nullptr, nullptr, out, st, h);
+    else
+        k_phase<EFSI_PF_UWCDI, 2><<<grid, block, 0, s>>>(P, U, V, phi, nullptr, nullptr, out, st, h);
 }
 
 }  // namespace efsi

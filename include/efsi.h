@@ -282,6 +282,12 @@ EFSI_API int efsi_project(efsi_handle* h, double* U, double* V, const double* ta
 EFSI_API int efsi_phase_field_rhs(efsi_handle* h, const double* U, const double* V, const double* phi,
                          const double* G, double* rhs);
 
+/* uwcdi_strang_step (PhaseFieldMethods.jl:810-850): dimensionally split UWCDI
+ * transport of phi over dt (half sweep, full sweep in the other direction, half
+ * sweep; x first when x_first != 0) for a context whose method is UWCDI. */
+EFSI_API int efsi_uwcdi_strang_step(efsi_handle* h, const double* U, const double* V, const double* phi,
+                           double dt, int32_t x_first, double* out);
+
 /* structure_tensor_rhs (StructureTensor.jl:377-463) with K_g built from G by the
  * context's growth-tensor model and the context's relaxation/extension. */
 EFSI_API int efsi_structure_tensor_rhs(efsi_handle* h, const double* sigma_xx, const double* sigma_yy,

@@ -26,7 +26,6 @@ EXTRA = {
     "relaxation_rhs": (None, [C.c_double, C.c_int32] + [_dp] * 6),
     "structure_tensor_diagnostics": (None, [C.c_int32] + [_dp] * 4),
     "body_force": (C.c_int32, [C.c_void_p, C.c_double, _dp, _dp]),
-    "uwcdi_strang_step": (C.c_int32, [C.c_void_p, _dp, _dp, _dp, C.c_double, C.c_int32, _dp]),
     "resource_explicit_rhs": (C.c_int32, [C.c_void_p] + [_dp] * 5),
     "constitutive_fields": (C.c_int32, [C.c_void_p] + [_dp] * 11),
     "divergence": (C.c_int32, [C.c_void_p, _dp, _dp, _dp]),

@@ -431,3 +431,33 @@ def test_mixed_precision_step_close_to_fp64(name):
         e = rel_err(getattr(b, f), getattr(a, f))
         assert e <= 1e-6, (f, e)
     assert sum(sb["velocity_iterations"]) > 0
+
+
+@pytest.mark.parametrize("normals", ["standard", "youngs", "smoothed9"])
+@pytest.mark.parametrize("periodic", [False, True])
+@pytest.mark.parametrize("x_first", [1, 0])
+def test_uwcdi_strang_step(normals, periodic, x_first):
+    """uwcdi_strang_step (PhaseFieldMethods.jl:810-850) on the GPU against the oracle,
+    and its phase mass against the input's (the reference's Strang test, runtests.jl)."""
+    method = ef.PirozzoliUWCDIPhaseField(1.0, normal_reconstruction=normals)
+    if periodic:
+        grid, metrics, bcs, models = periodic_problem(40, method)
+    else:
+        w = workloads.cavity_disk(N=40)
+        metrics, bcs = w.metrics, w.bcs
+        models = ef.FSIModels(viscosity=ef.ConstantViscosity(0.01), phase_field_method=method)
+    gpu, ora = pair(metrics, bcs, models, ef.IMEXNumerics())
+    inp = random_inputs(metrics, seed=5)
+    if periodic:
+        inp["U"][-1, :] = inp["U"][0, :]
+        inp["V"][:, -1] = inp["V"][:, 0]
+    else:
+        inp = _walls_consistent(inp, None)
+    outs = []
+    for h in (gpu, ora):
+        out = fz(metrics.Nx, metrics.Ny)
+        h.call("uwcdi_strang_step", dp(inp["U"]), dp(inp["V"]), dp(inp["phi"]), 0.002, x_first, dp(out))
+        outs.append(out)
+    assert rel_err(outs[0], outs[1]) <= OP_TOL
+    area = np.outer(metrics.dx_c, metrics.dy_c)
+    assert abs(np.sum(outs[0] * area) - np.sum(inp["phi"] * area)) <= 1e-12 * max(1.0, np.sum(inp["phi"] * area))
