@@ -442,6 +442,7 @@ void build_projection(efsi_handle* h, const efsi_config& cfg) {
     const double ax = h->P.g.hy / h->P.g.hx, ay = h->P.g.hx / h->P.g.hy;
     pj.nlev = (int)lv.size();
     pj.nsm = h->P.nsm;
+    pj.mixed = cfg.numerics.precision == EFSI_PRECISION_MIXED;
     for (int l = 0; l < pj.nlev; ++l) {
         MGLevel& M = pj.lev[l];
         const HostLevel& H = lv[l];
@@ -454,12 +455,19 @@ void build_projection(efsi_handle* h, const efsi_config& cfg) {
         M.cl = up(H.cl); M.cr = up(H.cr); M.cb = up(H.cb); M.ct = up(H.ct);
         size_t n = (size_t)H.nx * H.ny;
         M.x = h->dalloc<double>(n); M.xo = h->dalloc<double>(n); M.b = h->dalloc<double>(n); M.r = h->dalloc<double>(n);
+        if (pj.mixed) { M.xf = h->dalloc<float>(n); M.xof = h->dalloc<float>(n); M.bf = h->dalloc<float>(n); }
     }
     const HostLevel& C = lv.back();
     std::vector<double> inv = coarse_inverse(C, ax, ay, px, py, pj.nullspace);
     pj.nc = C.nx * C.ny;
     pj.coarse_inv = h->dalloc<double>(inv.size());
     check_cuda(cudaMemcpy(pj.coarse_inv, inv.data(), sizeof(double) * inv.size(), cudaMemcpyHostToDevice), "mg upload");
+    if (pj.mixed) {
+        std::vector<float> invf(inv.begin(), inv.end());
+        pj.coarse_inv_f = h->dalloc<float>(invf.size());
+        check_cuda(cudaMemcpy(pj.coarse_inv_f, invf.data(), sizeof(float) * invf.size(), cudaMemcpyHostToDevice),
+                   "mg upload");
+    }
     const size_t N = (size_t)Nx * Ny;
     pj.x = h->dalloc<double>(N); pj.r[0] = h->dalloc<double>(N); pj.r[1] = h->dalloc<double>(N); pj.z = pj.lev[0].xo;
     pj.p[0] = h->dalloc<double>(N); pj.p[1] = h->dalloc<double>(N);

@@ -858,7 +858,8 @@ __device__ __forceinline__ void rweights(int I, int nc, bool per, int (&f)[4], d
 }
 
 // Bilinear prolongation value (P e) at fine cell (i,j).
-__device__ __forceinline__ double prolong(const MGLevel& C, int px, int py, const double* e, int i, int j) {
+template <class E>
+__device__ __forceinline__ double prolong(const MGLevel& C, int px, int py, const E* e, int i, int j) {
     auto pair = [](int f, int nc, bool per, int& I0, int& I1) {
         I0 = f / 2;
         I1 = (f & 1) ? I0 + 1 : I0 - 1;
@@ -868,8 +869,8 @@ __device__ __forceinline__ double prolong(const MGLevel& C, int px, int py, cons
     int I0, I1, J0, J1;
     pair(i, C.nx, px, I0, I1);
     pair(j, C.ny, py, J0, J1);
-    auto E = [&](int a, int b) { return __ldg(e + cidx(a, b, C.nx)); };
-    return 0.75 * (0.75 * E(I0, J0) + 0.25 * E(I1, J0)) + 0.25 * (0.75 * E(I0, J1) + 0.25 * E(I1, J1));
+    auto Ev = [&](int a, int b) { return (double)__ldg(e + cidx(a, b, C.nx)); };
+    return 0.75 * (0.75 * Ev(I0, J0) + 0.25 * Ev(I1, J0)) + 0.25 * (0.75 * Ev(I0, J1) + 0.25 * Ev(I1, J1));
 }
 
 // ---- fused multigrid kernels ----------------------------------------------------------------
@@ -934,10 +935,13 @@ struct CGFuse {
 // at walls, wrap when periodic).  Writes L.x (needed by the up leg) and C.b.
 // FUSE: b is r_new of the CG update, formed on the fly over the halo; the owned cells
 // of r_new and x are written and |r_new|^2 decides convergence.
-template <int T, bool FUSE>
+// IN: element type of b (the finest level reads the FP64 CG residual); S: storage of
+// the level arrays (FP64, or FP32 in the precision form).  Arithmetic is FP64.
+template <int T, bool FUSE, class IN, class S>
 __global__ void __launch_bounds__(256, 4) k_mg_down(MGLevel L, MGLevel C, int px, int py,
-                                                    const double* __restrict__ b, CGFuse f, CGScal* cg, RedSlot rs,
-                                                    int* iters_out, cudaGraphConditionalHandle cond) {
+                                                    const IN* __restrict__ b, S* x_out, S* cb_out, CGFuse f,
+                                                    CGScal* cg, RedSlot rs, int* iters_out,
+                                                    cudaGraphConditionalHandle cond) {
     constexpr int H = 3, W = T + 2 * H;
     __shared__ double sb[W * W];  // b, then the residual (halo 1)
     __shared__ double sx[W * W];  // pre-smoothed x (valid within halo 2)
@@ -974,7 +978,7 @@ __global__ void __launch_bounds__(256, 4) k_mg_down(MGLevel L, MGLevel C, int px
                 k = cidx(sp.wi, sp.wj, nx);
                 lev_diag(L, px, py, sp.wi, sp.wj, vd[q]);
             }
-            vb[q] = FUSE ? __ldg(f.r_old + k) - a * __ldg(f.Ap + k) : __ldg(b + k);
+            vb[q] = FUSE ? __ldg(f.r_old + k) - a * __ldg(f.Ap + k) : (double)__ldg(b + k);
         }
 #pragma unroll
         for (int q = 0; q < NS; ++q) {
@@ -1052,13 +1056,13 @@ __global__ void __launch_bounds__(256, 4) k_mg_down(MGLevel L, MGLevel C, int px
                         if (wx[aa] != 0.0) row += wx[aa] * sb[(2 * cy + bb + 2) * W + 2 * cx + aa + 2];
                     sum += wy[bb] * row;
                 }
-                C.b[cidx(I, J, C.nx)] = sum;
+                cb_out[cidx(I, J, C.nx)] = (S)sum;
             }
         }
         for (int s = tid; s < T * T; s += 256) {
             const int lx = s % T, ly = s / T;
             const int gi = i0 + lx, gj = j0 + ly;
-            if (gi < nx && gj < L.ny) L.x[cidx(gi, gj, nx)] = sx[(ly + H) * W + lx + H];
+            if (gi < nx && gj < L.ny) x_out[cidx(gi, gj, nx)] = (S)sx[(ly + H) * W + lx + H];
         }
         __syncthreads();
     }
@@ -1076,10 +1080,10 @@ __global__ void __launch_bounds__(256, 4) k_mg_down(MGLevel L, MGLevel C, int px
 
 // Up leg of one level: x + P e (bilinear prolongation), then the post-smoothing
 // black-then-red Gauss-Seidel sweep; on the finest level also r.z for CG.
-template <int T, bool DOT>
-__global__ void __launch_bounds__(256, 4) k_mg_up(MGLevel L, MGLevel C, int px, int py,
-                                                  const double* __restrict__ x, const double* __restrict__ e,
-                                                  const double* __restrict__ b, double* xo, CGScal* cg, RedSlot rs) {
+template <int T, bool DOT, class S, class IN, class OUT>
+__global__ void __launch_bounds__(256, 4) k_mg_up(MGLevel L, MGLevel C, int px, int py, const S* __restrict__ x,
+                                                  const S* __restrict__ e, const IN* __restrict__ b, OUT* xo,
+                                                  CGScal* cg, RedSlot rs) {
     constexpr int H = 2, W = T + 2 * H;
     __shared__ double sx[W * W];
     __shared__ double sb[W * W];
@@ -1114,8 +1118,8 @@ __global__ void __launch_bounds__(256, 4) k_mg_up(MGLevel L, MGLevel C, int px, 
                 lev_diag(L, px, py, wi, wj, dv[q]);
             }
             const size_t k = cidx(wi, wj, nx);
-            xv[q] = __ldg(x + k) + prolong(C, px, py, e, wi, wj);
-            bv[q] = __ldg(b + k);
+            xv[q] = (double)__ldg(x + k) + prolong(C, px, py, e, wi, wj);
+            bv[q] = (double)__ldg(b + k);
         }
 #pragma unroll
         for (int q = 0; q < NS; ++q) {
@@ -1150,7 +1154,7 @@ __global__ void __launch_bounds__(256, 4) k_mg_up(MGLevel L, MGLevel C, int px, 
                 const double off = inner ? inner_off(L, sx, k, W) : slot_off(L, px, py, gi, gj, sx, k, W);
                 val = (bc + off) / sd[k];
             }
-            xo[cidx(gi, gj, nx)] = val;
+            xo[cidx(gi, gj, nx)] = (OUT)val;
             acc[0] += bc * val;
         }
         __syncthreads();
@@ -1164,8 +1168,8 @@ __global__ void __launch_bounds__(256, 4) k_mg_up(MGLevel L, MGLevel C, int px, 
 }
 
 // Coarsest level: x = Minv b with the dense (shifted) inverse; 8 rows per block.
-__global__ void k_mg_dense(int n, const double* __restrict__ Minv, const double* __restrict__ b, double* x,
-                           const CGScal* cg) {
+template <class S>
+__global__ void k_mg_dense(int n, const S* __restrict__ Minv, const S* __restrict__ b, S* x, const CGScal* cg) {
     if (cg && cg->done) return;
     __shared__ double sb[1024];
     for (int k = threadIdx.x; k < n; k += blockDim.x) sb[k] = b[k];
@@ -1176,7 +1180,7 @@ __global__ void k_mg_dense(int n, const double* __restrict__ Minv, const double*
         double s = 0.0;
         for (int k = lane; k < n; k += 32) s += Minv[(size_t)row * n + k] * sb[k];
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if (lane == 0) x[row] = s;
+        if (lane == 0) x[row] = (S)s;
     }
 }
 
@@ -1193,16 +1197,55 @@ __global__ void k_dot_rz(int n, const double* __restrict__ r, const double* __re
     }
 }
 
-// z = M r_fine with one V(1,1)-cycle; the finest down leg optionally carries the CG update.
-static void vcycle(const Projection& pj, const double* r_fine, const CGFuse* fuse, CGScal* cg, const RedSlot& rs,
-                   const RedSlot& rs2, int* iters_out, cudaGraphConditionalHandle cond, int px, int py,
-                   cudaStream_t s) {
-    const int n = pj.nlev;
-    if (n == 1) {
-        k_mg_dense<<<(pj.nc + 7) / 8, 256, 0, s>>>(pj.nc, pj.coarse_inv, r_fine, pj.z, cg);
-        k_dot_rz<<<(pj.nc + 255) / 256, 256, 0, s>>>(pj.nc, r_fine, pj.z, cg, rs2);
-        return;
+// Level arrays of storage type S (FP64, or FP32 in the precision form).
+template <class S> struct LevelArrays;
+template <> struct LevelArrays<double> {
+    static double* x(const MGLevel& L) { return L.x; }
+    static double* xo(const MGLevel& L) { return L.xo; }
+    static double* b(const MGLevel& L) { return L.b; }
+    static const double* inv(const Projection& p) { return p.coarse_inv; }
+};
+template <> struct LevelArrays<float> {
+    static float* x(const MGLevel& L) { return L.xf; }
+    static float* xo(const MGLevel& L) { return L.xof; }
+    static float* b(const MGLevel& L) { return L.bf; }
+    static const float* inv(const Projection& p) { return p.coarse_inv_f; }
+};
+
+template <int T, class S>
+static void mg_down(const MGLevel& L, const MGLevel& C, int l, const double* r_fine, const CGFuse* fuse, int grid,
+                    CGScal* cg, const RedSlot& rs, int* iters_out, cudaGraphConditionalHandle cond, int px, int py,
+                    cudaStream_t s) {
+    using A = LevelArrays<S>;
+    if (l == 0) {
+        if (fuse)
+            k_mg_down<T, true, double, S><<<grid, 256, 0, s>>>(L, C, px, py, r_fine, A::x(L), A::b(C), *fuse, cg, rs,
+                                                              iters_out, cond);
+        else
+            k_mg_down<T, false, double, S><<<grid, 256, 0, s>>>(L, C, px, py, r_fine, A::x(L), A::b(C), CGFuse{},
+                                                               cg, rs, nullptr, 0);
+    } else {
+        k_mg_down<T, false, S, S><<<grid, 256, 0, s>>>(L, C, px, py, A::b(L), A::x(L), A::b(C), CGFuse{}, cg, rs,
+                                                       nullptr, 0);
     }
+}
+
+template <int T, class S>
+static void mg_up(const Projection& pj, const MGLevel& L, const MGLevel& C, int l, const double* r_fine, int grid,
+                  CGScal* cg, const RedSlot& rs2, int px, int py, cudaStream_t s) {
+    using A = LevelArrays<S>;
+    if (l == 0)
+        k_mg_up<T, true, S, double, double><<<grid, 256, 0, s>>>(L, C, px, py, A::x(L), A::xo(C), r_fine, pj.z, cg,
+                                                                rs2);
+    else
+        k_mg_up<T, false, S, S, S><<<grid, 256, 0, s>>>(L, C, px, py, A::x(L), A::xo(C), A::b(L), A::xo(L), cg, rs2);
+}
+
+template <class S>
+static void vcycle_levels(const Projection& pj, const double* r_fine, const CGFuse* fuse, CGScal* cg,
+                          const RedSlot& rs, const RedSlot& rs2, int* iters_out, cudaGraphConditionalHandle cond,
+                          int px, int py, cudaStream_t s) {
+    const int n = pj.nlev;
     // 32x32 tiles while they fill the device, 16x16 below (shorter dependent chains)
     auto wide = [&](const MGLevel& L) { return ((L.nx + 31) / 32) * ((L.ny + 31) / 32) >= pj.nsm; };
     auto grid = [&](const MGLevel& L, int T) {
@@ -1210,47 +1253,44 @@ static void vcycle(const Projection& pj, const double* r_fine, const CGFuse* fus
     };
     for (int l = 0; l + 1 < n; ++l) {
         const MGLevel &L = pj.lev[l], &C = pj.lev[l + 1];
-        const double* b = l == 0 ? r_fine : L.b;
-        const bool fz = l == 0 && fuse;
-        const CGFuse fa = fz ? *fuse : CGFuse{};
-        if (wide(L)) {
-            if (fz) k_mg_down<32, true><<<grid(L, 32), 256, 0, s>>>(L, C, px, py, b, fa, cg, rs, iters_out, cond);
-            else k_mg_down<32, false><<<grid(L, 32), 256, 0, s>>>(L, C, px, py, b, fa, cg, rs, nullptr, 0);
-        } else {
-            if (fz) k_mg_down<16, true><<<grid(L, 16), 256, 0, s>>>(L, C, px, py, b, fa, cg, rs, iters_out, cond);
-            else k_mg_down<16, false><<<grid(L, 16), 256, 0, s>>>(L, C, px, py, b, fa, cg, rs, nullptr, 0);
-        }
+        if (wide(L)) mg_down<32, S>(L, C, l, r_fine, fuse, grid(L, 32), cg, rs, iters_out, cond, px, py, s);
+        else mg_down<16, S>(L, C, l, r_fine, fuse, grid(L, 16), cg, rs, iters_out, cond, px, py, s);
     }
     const MGLevel& B = pj.lev[n - 1];
-    k_mg_dense<<<(pj.nc + 7) / 8, 256, 0, s>>>(pj.nc, pj.coarse_inv, B.b, B.xo, cg);
+    using A = LevelArrays<S>;
+    k_mg_dense<S><<<(pj.nc + 7) / 8, 256, 0, s>>>(pj.nc, A::inv(pj), A::b(B), A::xo(B), cg);
     for (int l = n - 2; l >= 0; --l) {
         const MGLevel &L = pj.lev[l], &C = pj.lev[l + 1];
-        const double* b = l == 0 ? r_fine : L.b;
-        double* out = l == 0 ? pj.z : L.xo;
-        if (wide(L)) {
-            if (l == 0) k_mg_up<32, true><<<grid(L, 32), 256, 0, s>>>(L, C, px, py, L.x, C.xo, b, out, cg, rs2);
-            else k_mg_up<32, false><<<grid(L, 32), 256, 0, s>>>(L, C, px, py, L.x, C.xo, b, out, cg, rs2);
-        } else {
-            if (l == 0) k_mg_up<16, true><<<grid(L, 16), 256, 0, s>>>(L, C, px, py, L.x, C.xo, b, out, cg, rs2);
-            else k_mg_up<16, false><<<grid(L, 16), 256, 0, s>>>(L, C, px, py, L.x, C.xo, b, out, cg, rs2);
-        }
+        if (wide(L)) mg_up<32, S>(pj, L, C, l, r_fine, grid(L, 32), cg, rs2, px, py, s);
+        else mg_up<16, S>(pj, L, C, l, r_fine, grid(L, 16), cg, rs2, px, py, s);
     }
+}
+
+// z = M r_fine with one V(1,1)-cycle; the finest down leg optionally carries the CG update.
+static void vcycle(const Projection& pj, const double* r_fine, const CGFuse* fuse, CGScal* cg, const RedSlot& rs,
+                   const RedSlot& rs2, int* iters_out, cudaGraphConditionalHandle cond, int px, int py,
+                   cudaStream_t s) {
+    if (pj.nlev == 1) {
+        k_mg_dense<double><<<(pj.nc + 7) / 8, 256, 0, s>>>(pj.nc, pj.coarse_inv, r_fine, pj.z, cg);
+        k_dot_rz<<<(pj.nc + 255) / 256, 256, 0, s>>>(pj.nc, r_fine, pj.z, cg, rs2);
+        return;
+    }
+    if (pj.mixed) vcycle_levels<float>(pj, r_fine, fuse, cg, rs, rs2, iters_out, cond, px, py, s);
+    else vcycle_levels<double>(pj, r_fine, fuse, cg, rs, rs2, iters_out, cond, px, py, s);
 }
 
 int proj_update_vcycle_kernels(const Projection& pj) { return pj.nlev == 1 ? 3 : 2 * (pj.nlev - 1) + 1; }
 int proj_init_kernels(const Projection& pj) { return 1 + (pj.nlev == 1 ? 2 : 2 * (pj.nlev - 1) + 1); }
 double proj_update_vcycle_bytes(const Projection& pj) {
-    double w = 0.0;
     const double n0 = (double)pj.lev[0].nx * pj.lev[0].ny;
-    if (pj.nlev == 1) {
-        w = 6.0 * n0 + (double)pj.nc * pj.nc + 4.0 * pj.nc;
-    } else {
-        // finest: r_old, Kp, p, x read; x, r_new, L.x written; C.b; up: L.x, e, r_new read, z written
-        w = 10.5 * n0;
-        for (int l = 1; l + 1 < pj.nlev; ++l) w += 5.5 * (double)pj.lev[l].nx * pj.lev[l].ny;
-        w += (double)pj.nc * pj.nc + 2.0 * pj.nc;
-    }
-    return 8.0 * w;
+    if (pj.nlev == 1) return 8.0 * (6.0 * n0 + (double)pj.nc * pj.nc + 4.0 * pj.nc);
+    const double e = pj.mixed ? 4.0 : 8.0;  // bytes of a multigrid level element
+    // finest: r_old, Kp, p, x read and x, r_new written (FP64); L.x and C.b written;
+    // up: L.x, e read, r_new read (FP64), z written (FP64)
+    double b = 8.0 * 8.0 * n0 + e * (2.25 * n0 + 0.25 * n0 + 1.0 * n0);
+    for (int l = 1; l + 1 < pj.nlev; ++l) b += e * 5.5 * (double)pj.lev[l].nx * pj.lev[l].ny;
+    b += e * ((double)pj.nc * pj.nc + 2.0 * pj.nc);
+    return b;
 }
 
 // ---- right-hand side (Projection.jl:198-221) -----------------------------------------------

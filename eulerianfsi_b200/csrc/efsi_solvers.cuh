@@ -65,13 +65,16 @@ struct MGLevel {
     double ax, ay;                      // hy/hx, hx/hy (same on every level)
     double *cl, *cr, *cb, *ct;          // boundary coefficient factor per boundary cell (device)
     double *x, *xo, *b, *r;             // level vectors (x/xo ping-pong)
+    float *xf, *xof, *bf;               // the same in FP32 (precision form)
 };
 struct Projection {
     int nlev;
     MGLevel lev[16];
     double* coarse_inv;   // dense inverse of the coarsest operator (shifted when singular)
+    float* coarse_inv_f;  // its FP32 copy (precision form)
     int nc;
     bool nullspace;
+    bool mixed;           // precision form: multigrid levels stored and applied in FP32
     int nsm;              // multiprocessors (persistent launch grids)
     // fine-level CG vectors (r ping-pongs between iterations when multigrid levels exist)
     double *x, *r[2], *z, *p[2], *Ap, *b, *rhs;
