@@ -114,6 +114,35 @@ class Stats(Structure):
                 ("site_bytes", c_double)]
 
 
+DIAG_MAX_MODES = 8
+
+
+class DiagConfig(Structure):
+    _fields_ = [("density", c_double), ("elastic_modulus", c_double), ("sigma_core_cutoff", c_double),
+                ("sigma_interface_cutoff", c_double), ("sigma_safety_cutoff", c_double),
+                ("h_interface", c_double), ("nmax", c_int32), ("reserved", c_int32 * 3)]
+
+
+class TensorRegion(Structure):
+    _fields_ = [("cells", c_int64)] + [(n, c_double) for n in (
+        "area", "determinant_min", "determinant_max", "max_abs_determinant_error",
+        "mean_abs_determinant_error", "lambda_min", "lambda_max")] + [
+        ("non_spd_cells", c_int64), ("max_effective_stress", c_double), ("mean_effective_stress", c_double)]
+
+
+class Diagnostics(Structure):
+    _fields_ = [(n, c_double) for n in (
+        "x_centroid", "y_centroid", "phase_integral", "perimeter_proxy", "mixed_layer_measure",
+        "effective_interface_width", "effective_interface_cells", "covariance_major", "covariance_minor",
+        "aspect_ratio", "orientation_radians", "R0")] + [
+        ("Rc", c_double * DIAG_MAX_MODES), ("Rs", c_double * DIAG_MAX_MODES),
+        ("amplitudes", c_double * DIAG_MAX_MODES)] + [(n, c_double) for n in (
+            "phi_minimum", "phi_maximum", "lower_violation", "upper_violation")] + [
+        ("out_of_bounds_cells", c_int64)] + [(n, c_double) for n in (
+            "maximum_speed", "kinetic_energy", "divergence_linf", "divergence_l2", "max_abs_U", "max_abs_V")] + [
+        ("tensor", TensorRegion * 4)]
+
+
 SITES = ["phase", "momentum", "structure", "visc_apply", "visc_cg", "visc_init", "pcg_matvec",
          "pcg_update", "vcycle", "proj_rhs", "proj_finish", "combine", "vel_rhs", "finalize"]
 
@@ -138,6 +167,7 @@ SIGNATURES = {
     "apply_viscous_operator": (c_int32, [_H, _dp, _dp, _dp]),
     "get_stats": (c_int32, [_H, POINTER(Stats)]),
     "uwcdi_strang_step": (c_int32, [_H, _dp, _dp, _dp, c_double, c_int32, _dp]),
+    "state_diagnostics": (c_int32, [_H, POINTER(DiagConfig), POINTER(Diagnostics)]),
 }
 CUDA_ONLY = {
     "set_timed_site": (c_int32, [_H, c_int32]),

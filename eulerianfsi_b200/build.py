@@ -15,8 +15,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libefsi.so")
-SOURCES = ["efsi_ops.cu", "efsi_phase.cu", "efsi_solvers.cu", "efsi_api.cu"]
-HEADERS = ["efsi_common.cuh", "efsi_device.cuh", "efsi_kernels.cuh", "efsi_solvers.cuh"]
+SOURCES = ["efsi_ops.cu", "efsi_phase.cu", "efsi_solvers.cu", "efsi_diag.cu", "efsi_api.cu"]
+HEADERS = ["efsi_common.cuh", "efsi_device.cuh", "efsi_kernels.cuh", "efsi_solvers.cuh", "efsi_diag.cuh"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-fvisibility=hidden", "-diag-suppress", "177"]

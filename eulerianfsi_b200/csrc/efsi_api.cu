@@ -22,6 +22,7 @@
 #include <string>
 #include <vector>
 
+#include "efsi_diag.cuh"
 #include "efsi_kernels.cuh"
 #include "efsi_solvers.cuh"
 
@@ -99,6 +100,11 @@ struct efsi_handle {
     DevBlock* host = nullptr;  // pinned mirror
     int* done_pinned = nullptr;
     RedSlot slot[8];
+    // driver diagnostics: reduction slots sized for 32 values, device totals, pinned copy
+    static constexpr int kDiagBlocks = 1024;
+    RedSlot dslot[3];
+    double* diag_dev = nullptr;
+    double* diag_pinned = nullptr;
     // solver batch predictions (host-driven mode)
     int pred[3] = {4, 4, 4};
     long long launches = 0;
@@ -140,6 +146,7 @@ struct efsi_handle {
         if (host) cudaFreeHost(host);
         if (done_pinned) cudaFreeHost(done_pinned);
         if (times_pinned) cudaFreeHost(times_pinned);
+        if (diag_pinned) cudaFreeHost(diag_pinned);
         if (hist_pinned) cudaFreeHost(hist_pinned);
         if (stream2) cudaStreamDestroy(stream2);
         if (stream) cudaStreamDestroy(stream);
@@ -1074,6 +1081,13 @@ int efsi_create(const efsi_config* cfg, efsi_handle** out) {
         check_cuda(cudaMallocHost(&h->host, sizeof(DevBlock)), "pinned");
         check_cuda(cudaMallocHost(&h->done_pinned, 4 * sizeof(int)), "pinned");
         std::memset(h->host, 0, sizeof(DevBlock));
+        for (RedSlot& r : h->dslot) {
+            r.part = h->dalloc<double>((size_t)efsi_handle::kDiagBlocks * 32);
+            r.ticket = h->dalloc<unsigned>(1);
+            r.maxBlocks = efsi_handle::kDiagBlocks;
+        }
+        h->diag_dev = h->dalloc<double>(kDiagTotals);
+        check_cuda(cudaMallocHost(&h->diag_pinned, kDiagTotals * sizeof(double)), "pinned");
         h->times_dev = h->dalloc<double>(2 * (size_t)kMaxBatch);
         h->hist_dev = h->dalloc<StepRec>(kMaxBatch);
         check_cuda(cudaMallocHost(&h->times_pinned, 2 * (size_t)kMaxBatch * sizeof(double)), "pinned");
@@ -1349,6 +1363,72 @@ int efsi_apply_viscous_operator(efsi_handle* h, const double* phi, const double*
         d2h(h, out, h->Iu[0], h->nc);
         d2h(h, out + h->nc, h->Iv[0], h->nc);
         check_cuda(cudaStreamSynchronize(h->stream), "apply_viscous_operator");
+    });
+}
+
+int efsi_state_diagnostics(efsi_handle* h, const efsi_diag_config* cfg, efsi_diagnostics* out) {
+    return guarded(h, [&] {
+        if (!cfg || !out) throw Err{EFSI_ARG, "config and out must not be NULL"};
+        if (cfg->nmax < 0 || cfg->nmax > EFSI_DIAG_MAX_MODES) throw Err{EFSI_ARG, "nmax must lie in 0..8"};
+        launch_diagnostics(h->P, *cfg, h->U, h->V, h->phi, h->sxx, h->syy, h->sxy, h->dslot[0], h->dslot[1],
+                           h->dslot[2], h->diag_dev, efsi_handle::kDiagBlocks, h->stream);
+        check_cuda(cudaGetLastError(), "diagnostics");
+        d2h(h, h->diag_pinned, h->diag_dev, kDiagTotals);
+        check_cuda(cudaStreamSynchronize(h->stream), "diagnostics");
+        const double* S = h->diag_pinned;
+        const double* M = S + kDiagSums;
+        const double* S2 = M + kDiagMaxes;
+        const double eps = 2.220446049250313e-16, pi = 3.14159265358979323846, nan = std::nan("");
+        const double mass = S[0];
+        // phase_centroid (run_sugiyama_lid_driven_cavity.jl:497-498)
+        if (!(mass > eps)) throw Err{EFSI_ARG, "Phase integral is too small to define a centroid."};
+        efsi_diagnostics& o = *out;
+        o = efsi_diagnostics{};
+        o.x_centroid = S[1] / mass;
+        o.y_centroid = S[2] / mass;
+        o.phase_integral = mass;
+        o.perimeter_proxy = S[3];
+        o.mixed_layer_measure = S[4];
+        // phase_geometry_diagnostics (:673-688)
+        const double cxx = S2[0] / mass, cyy = S2[1] / mass, cxy = S2[2] / mass;
+        const double gap = std::hypot(cxx - cyy, 2.0 * cxy);
+        o.covariance_major = 0.5 * (cxx + cyy + gap);
+        o.covariance_minor = 0.5 * (cxx + cyy - gap);
+        o.aspect_ratio = o.covariance_minor > 0.0 ? std::sqrt(o.covariance_major / o.covariance_minor) : INFINITY;
+        o.orientation_radians = gap > 100.0 * eps ? 0.5 * std::atan2(2.0 * cxy, cxx - cyy) : 0.0;
+        o.R0 = S[3] / (2.0 * pi);
+        o.effective_interface_width = S[3] > eps ? S[4] / S[3] : nan;
+        o.effective_interface_cells = o.effective_interface_width / cfg->h_interface;
+        for (int n = 0; n < cfg->nmax; ++n) {
+            o.Rc[n] = S2[3 + n];
+            o.Rs[n] = S2[3 + EFSI_DIAG_MAX_MODES + n];
+            o.amplitudes[n] = std::hypot(o.Rc[n], o.Rs[n]);
+        }
+        // phase_bound_diagnostics (:709-722)
+        o.phi_minimum = -M[0];
+        o.phi_maximum = M[1];
+        o.lower_violation = std::max(0.0, -o.phi_minimum);
+        o.upper_violation = std::max(0.0, o.phi_maximum - 1.0);
+        o.out_of_bounds_cells = (int64_t)S[8];
+        // flow_diagnostics (:724-749) and the inputs of comparison_timestep_bounds
+        o.maximum_speed = M[2];
+        o.kinetic_energy = S[5];
+        o.divergence_linf = M[3];
+        o.divergence_l2 = std::sqrt(S[6] / S[7]);
+        o.max_abs_U = M[4];
+        o.max_abs_V = M[5];
+        // tensor_region_diagnostics (:739-804)
+        for (int r = 0; r < 4; ++r) {
+            const double* s = S + 9 + 5 * r;
+            const double* m = M + 6 + 6 * r;
+            efsi_tensor_region& g = o.tensor[r];
+            if (s[0] == 0.0 || s[1] == 0.0) {
+                g = efsi_tensor_region{0, 0.0, nan, nan, nan, nan, nan, nan, 0, nan, nan};
+            } else {
+                g = efsi_tensor_region{(int64_t)s[0], s[1], -m[0], m[1], m[2], s[2] / s[1], -m[3], m[4],
+                                       (int64_t)s[4], m[5], s[3] / s[1]};
+            }
+        }
     });
 }
 

@@ -225,6 +225,48 @@ typedef struct efsi_stats {
                                            writes once, FP64)                            */
 } efsi_stats;
 
+/* Driver diagnostics of the cavity benchmarks (run_sugiyama_lid_driven_cavity.jl),
+ * computed on the device-resident state so that a time loop needs no state
+ * download per step. */
+#define EFSI_DIAG_MAX_MODES 8
+typedef struct efsi_diag_config {
+    double  density;                 /* flow_diagnostics kinetic-energy density        */
+    double  elastic_modulus;         /* tensor_cell_diagnostics_2d                      */
+    double  sigma_core_cutoff;       /* tensor regions: core phi >= core,               */
+    double  sigma_interface_cutoff;  /*   interface in (interface, core),               */
+    double  sigma_safety_cutoff;     /*   tail in (safety, interface]                   */
+    double  h_interface;             /* effective_interface_cells = width / h_interface */
+    int32_t nmax;                    /* boundary Fourier modes, 0..EFSI_DIAG_MAX_MODES  */
+    int32_t reserved[3];
+} efsi_diag_config;
+
+/* tensor_region_diagnostics (:739-804); NaN fields when the region is empty. */
+typedef struct efsi_tensor_region {
+    int64_t cells;
+    double  area, determinant_min, determinant_max, max_abs_determinant_error,
+            mean_abs_determinant_error, lambda_min, lambda_max;
+    int64_t non_spd_cells;
+    double  max_effective_stress, mean_effective_stress;
+} efsi_tensor_region;
+
+typedef struct efsi_diagnostics {
+    /* phase_centroid + phase_geometry_diagnostics (:488-507, :615-707); cell
+     * centres at ((i+1/2) Lx/Nx, (j+1/2) Ly/Ny) */
+    double x_centroid, y_centroid, phase_integral, perimeter_proxy, mixed_layer_measure,
+           effective_interface_width, effective_interface_cells, covariance_major,
+           covariance_minor, aspect_ratio, orientation_radians, R0;
+    double Rc[EFSI_DIAG_MAX_MODES], Rs[EFSI_DIAG_MAX_MODES], amplitudes[EFSI_DIAG_MAX_MODES];
+    /* phase_bound_diagnostics (:709-722) */
+    double  phi_minimum, phi_maximum, lower_violation, upper_violation;
+    int64_t out_of_bounds_cells;
+    /* flow_diagnostics (:724-749) */
+    double maximum_speed, kinetic_energy, divergence_linf, divergence_l2;
+    /* inputs of comparison_timestep_bounds (:852-934): max |U|, max |V| over all faces */
+    double max_abs_U, max_abs_V;
+    /* tensor_diagnostics_detailed (:806-828): global, core, interface, tail */
+    efsi_tensor_region tensor[4];
+} efsi_diagnostics;
+
 typedef struct efsi_handle efsi_handle;
 
 /* build_imex_context + allocate_imex_workspace (TimeIntegrationIMEX.jl:468-493,
@@ -310,6 +352,12 @@ EFSI_API int efsi_apply_viscous_operator(efsi_handle* h, const double* phi, cons
                                 double* out);
 
 EFSI_API int efsi_get_stats(const efsi_handle* h, efsi_stats* stats);
+
+/* The diagnostics above for the device-resident state (the state after the last
+ * efsi_integrate_step / efsi_step_n / efsi_upload_state).  Driver-side reductions of
+ * run_sugiyama_lid_driven_cavity.jl:488-828; the phase gradient of the perimeter
+ * proxy uses the context's phi boundaries (phase_center_gradient, :600-613). */
+EFSI_API int efsi_state_diagnostics(efsi_handle* h, const efsi_diag_config* config, efsi_diagnostics* out);
 
 /* Bracket every launch of one EFSI_SITE_* with CUDA events on the handle's stream
  * (EFSI_SITE_NONE switches timing off) and reset the site accumulators of

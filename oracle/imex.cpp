@@ -639,6 +639,18 @@ int oracle_constitutive_fields(Ctx* h, const double* phi, const double* c, doubl
     });
 }
 
+int oracle_state_diagnostics(Ctx* h, const efsi_diag_config* cfg, efsi_diagnostics* out) {
+    return guarded(h, [&] {
+        if (!cfg || !out) arg_error("config and out must not be NULL");
+        state_diagnostics(h->m, h->bphi, h->U, h->V, h->phi, h->sxx, h->syy, h->sxy, *cfg, *out);
+    });
+}
+
+int oracle_tensor_cell_diagnostics(double sxx, double syy, double sxy, double phi, double modulus, double* out) {
+    tensor_cell_diagnostics(sxx, syy, sxy, phi, modulus, out);
+    return 0;
+}
+
 int oracle_divergence(Ctx* h, const double* U, const double* V, double* out) {
     return guarded(h, [&] {
         const int Nx = h->m.Nx, Ny = h->m.Ny;

@@ -129,6 +129,12 @@ void relaxation_rhs(const efsi_models& md, double sxx, double syy, double sxy,
                     double& rxx, double& ryy, double& rxy);                    // StructuralConstitutive.jl:61-85
 
 // ---- solvers ----------------------------------------------------------------
+// Cavity-driver diagnostics (run_sugiyama_lid_driven_cavity.jl:484-828).
+void state_diagnostics(const Mesh& m, const BCS& bphi, const F2& U, const F2& V, const F2& phi, const F2& sxx,
+                       const F2& syy, const F2& sxy, const efsi_diag_config& cfg, efsi_diagnostics& out);
+// tensor_cell_diagnostics_2d (BenchmarkUtilities.jl:62-87): det, det-1, lambda_min, lambda_max, stress.
+void tensor_cell_diagnostics(double sxx, double syy, double sxy, double phi, double modulus, double out[5]);
+
 struct Projector;
 struct ProjOut { double linear_relative_residual, constraint_linf, constraint_l2, compatibility_defect; int iters; };
 Projector* make_projector(const Mesh& m, const BCS& bq);

@@ -29,6 +29,7 @@ EXTRA = {
     "resource_explicit_rhs": (C.c_int32, [C.c_void_p] + [_dp] * 5),
     "constitutive_fields": (C.c_int32, [C.c_void_p] + [_dp] * 11),
     "divergence": (C.c_int32, [C.c_void_p, _dp, _dp, _dp]),
+    "tensor_cell_diagnostics": (C.c_int32, [C.c_double] * 5 + [_dp]),
 }
 
 _LIB = None

@@ -17,7 +17,8 @@ STRUCTS = {
     "efsi_bc_side": _abi.BCSide, "efsi_bc_setup": _abi.BCSetup, "efsi_mesh": _abi.Mesh,
     "efsi_models": _abi.Models, "efsi_numerics": _abi.Numerics, "efsi_config": _abi.Config,
     "efsi_step_report": _abi.StepReportC, "efsi_projection_result": _abi.ProjectionResultC,
-    "efsi_stats": _abi.Stats,
+    "efsi_stats": _abi.Stats, "efsi_diag_config": _abi.DiagConfig, "efsi_tensor_region": _abi.TensorRegion,
+    "efsi_diagnostics": _abi.Diagnostics,
 }
 
 

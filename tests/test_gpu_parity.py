@@ -461,3 +461,39 @@ def test_uwcdi_strang_step(normals, periodic, x_first):
     assert rel_err(outs[0], outs[1]) <= OP_TOL
     area = np.outer(metrics.dx_c, metrics.dy_c)
     assert abs(np.sum(outs[0] * area) - np.sum(inp["phi"] * area)) <= 1e-12 * max(1.0, np.sum(inp["phi"] * area))
+
+
+@pytest.mark.parametrize("name", ["cavity_disk", "filament"])
+def test_state_diagnostics_match_oracle(name):
+    """Device-side driver diagnostics (run_sugiyama_lid_driven_cavity.jl:484-828)
+    against the oracle's restatement, on a state advanced by two steps."""
+    from eulerianfsi_b200 import diagnostics
+    w = workloads.cavity_disk(N=48) if name == "cavity_disk" else workloads.filament_kolmogorov(N=40)
+    gpu, ora = pair(w.metrics, w.bcs, w.models, tight(w.numerics))
+    cfg = diagnostics.DiagnosticsConfig(elastic_modulus=0.1, sigma_core_cutoff=0.9, sigma_interface_cutoff=0.1,
+                                        sigma_safety_cutoff=1e-6, h_interface=1.0 / 48, nmax=6)
+    res = []
+    for h in (gpu, ora):
+        h.upload(w.state)
+        h.set_correction(fz(w.metrics.Nx, w.metrics.Ny))
+        for k in range(2):
+            h.call("integrate_step", k * w.dt, w.dt, None)
+        res.append(diagnostics.state_diagnostics(h, cfg))
+    g, o = res
+
+    def close(a, b, path):
+        if isinstance(b, dict):
+            for k in b:
+                close(a[k], b[k], path + "." + k)
+        elif isinstance(b, list):
+            for k, (x, y) in enumerate(zip(a, b)):
+                close(x, y, f"{path}[{k}]")
+        elif isinstance(b, int):
+            assert a == b, path
+        elif np.isnan(b):
+            assert np.isnan(a), path
+        else:
+            assert abs(a - b) <= 1e-10 * max(1.0, abs(b)), (path, a, b)
+
+    close(g, o, "diag")
+    assert g["global_region"]["cells"] == w.metrics.Nx * w.metrics.Ny

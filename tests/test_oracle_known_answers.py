@@ -342,3 +342,29 @@ def test_no_growth_rest_state():
     assert np.all(state.resource == 0.0)
     assert np.max(np.abs(state.U)) < 1e-9 and np.max(np.abs(state.V)) < 1e-9
     assert np.max(np.abs(state.phi - 0.5)) < 1e-9
+
+
+def test_tensor_cell_diagnostics_known_answer():
+    """tensor_cell_diagnostics_2d (test/runtests.jl:140-145)."""
+    from oracle.oracle import load
+    out = (C.c_double * 5)()
+    load().oracle_tensor_cell_diagnostics(2.0, 0.5, 0.0, 0.2, 10.0, out)
+    det, err, lmin, lmax, stress = list(out)
+    assert det == pytest.approx(1.0) and err == pytest.approx(0.0, abs=1e-15)
+    assert lmin == pytest.approx(0.5) and lmax == pytest.approx(2.0) and stress > 0.0
+
+
+def test_oracle_state_diagnostics_disk():
+    """Oracle diagnostics of a sharp disk: centroid at the disk centre, a perimeter
+    proxy near 2 pi r, and round covariance."""
+    from eulerianfsi_b200 import diagnostics, workloads
+    from eulerianfsi_b200.imex import ConfigBlock, Handle
+    from oracle.oracle import load
+    w = workloads.cavity_disk(N=64)
+    h = Handle(load(), "oracle_", ConfigBlock(w.metrics, w.bcs, w.models, w.numerics), w.metrics)
+    h.upload(w.state)
+    d = diagnostics.state_diagnostics(h, diagnostics.DiagnosticsConfig(nmax=4))
+    assert abs(d["x_centroid"] - 0.6) < 1e-3 and abs(d["y_centroid"] - 0.5) < 1e-3
+    assert abs(d["perimeter_proxy"] - 2 * np.pi * 0.2) / (2 * np.pi * 0.2) < 0.05
+    assert d["aspect_ratio"] < 1.01 and max(d["amplitudes"]) < 1e-2 * d["perimeter_proxy"]
+    assert d["global_region"]["cells"] == 64 * 64 and d["global_region"]["non_spd_cells"] == 0
