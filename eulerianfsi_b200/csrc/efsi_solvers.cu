@@ -44,8 +44,15 @@ struct CompactUV {
 // Matrix part of the viscous operator (no boundary data), rows u(i,j) and v(i,j).
 // INT: (i,j) is at least one cell away from every edge, so no boundary branch is
 // taken (the same arithmetic as the general path there, without its tests).
-template <bool INT, class X>
-__device__ __forceinline__ void visc_A(const Params& P, const MuField& mu, const X& x, int i, int j, double& au,
+// Constant viscosity known to the compiler (the common case: ConstantViscosity).
+struct MuConst {
+    double m;
+    __device__ __forceinline__ double c(int, int) const { return m; }
+    __device__ __forceinline__ double k(int, int) const { return m; }
+};
+
+template <bool INT, class X, class MU>
+__device__ __forceinline__ void visc_A(const Params& P, const MU& mu, const X& x, int i, int j, double& au,
                                        double& av) {
     const int Nx = P.g.Nx, Ny = P.g.Ny;
     const double ihx = P.g.ihx, ihy = P.g.ihy;
@@ -217,12 +224,21 @@ __device__ __forceinline__ void visc_halo_slot(int h, int& lx, int& ly) {
     else { int t = h - 2 * VSX; lx = t < VTY ? 0 : VSX - 1; ly = 1 + (t % VTY); }
 }
 
+// A u at (i,j) from a staged tile; interior points of a constant-viscosity model take
+// the specialised form (same arithmetic, viscosity known to the compiler).
+__device__ __forceinline__ void visc_A_tile(const Params& P, const double* phi, const TileUV& t, int i, int j,
+                                            double& au, double& av) {
+    if (P.md.viscosity == EFSI_VISC_CONSTANT && i >= 1 && i <= P.g.Nx - 2 && j >= 1 && j <= P.g.Ny - 2)
+        visc_A<true>(P, MuConst{P.md.viscosity_fluid}, t, i, j, au, av);
+    else
+        visc_A_any(P, make_mu(P, phi), t, i, j, au, av);
+}
+
 // w = u - alpha*A u at the thread's own point from the staged tile (0 on Dirichlet rows).
 __device__ __forceinline__ void visc_apply_tile(const Params& P, double alpha, const double* phi, const TileUV& t,
                                                 int i, int j, double un, double vn, double& w1, double& w2) {
-    MuField mu = make_mu(P, phi);
     double au, av;
-    visc_A_any(P, mu, t, i, j, au, av);
+    visc_A_tile(P, phi, t, i, j, au, av);
     w1 = u_fixed(P, i) ? 0.0 : un - alpha * au;
     w2 = v_fixed(P, j) ? 0.0 : vn - alpha * av;
 }
@@ -533,7 +549,7 @@ __global__ void __launch_bounds__(VTX * VTY, 3) k_visc_mx(Params P, DtCoef ac, d
             TileUV tl{su, sv, i0, j0, Nx, Ny};
             MuField mu = make_mu(P, phi);
             double au, av;
-            visc_A_any(P, mu, tl, i, j, au, av);
+            visc_A_tile(P, phi, tl, i, j, au, av);
             if (phase == MX_REFINE) {
                 if (START) {
                     double du, dv;
