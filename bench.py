@@ -111,6 +111,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(value: float, dist, device: str) -> float:
+    """The largest `value` over all ranks (every rank gets it); identity without
+    a process group.  Device times of replicas are combined this way."""
+    if dist is None:
+        return value
+    import torch
+    tt = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
 def build_workload(args, precision):
     from eulerianfsi_b200 import workloads
     return workloads.cavity_disks20(N=args.N, steps=args.steps, projection_reltol=args.projection_reltol,
@@ -199,11 +210,7 @@ def run_ours(args, rank, world, local_rank):
         if dist:
             dist.barrier()
         st = h.stats()
-        ms = st["device_ms"]
-        if dist:
-            tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms = float(tt.item())
+        ms = max_over_ranks(st["device_ms"], dist, "cuda")
         return dict(w=w, ctx=ctx, h=h, dts=dts, t=t + args.steps * w.dt, ms=ms, st=st, clocks=clocks)
 
     other = "fp64" if args.precision == "mixed" else "mixed"
@@ -259,10 +266,7 @@ def run_ours(args, rank, world, local_rank):
     for k in range(e2e_steps):
         ef.integrate_step(state, (k + 1) * w.dt, w.dt, ctx, work)
         e2e_ms += h.stats()["device_ms"]
-    if dist:
-        tt = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = max_over_ranks(e2e_ms, dist, "cuda")
     field_bytes = sum(a.nbytes for a in state.arrays())
     h2d = field_bytes + qpin.nbytes
     d2h = field_bytes + qpin.nbytes
