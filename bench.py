@@ -303,6 +303,57 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+CONFIGS = {  # the four benchmark configurations: workload builder and steps timed
+    "c0_cavity_disk_64": (lambda prec: _wl().cavity_disk(N=64, precision=prec), 50),
+    "c1_filament_256": (lambda prec: _wl().filament_kolmogorov(N=256, precision=prec), 50),
+    "c2_cavity_disks20_1024": (lambda prec: _wl().cavity_disks20(N=1024, precision=prec), 20),
+    "c3_channel_growth_1024x512": (lambda prec: _wl().channel_growth(N=512, precision=prec), 20),
+}
+
+
+def _wl():
+    from eulerianfsi_b200 import workloads
+    return workloads
+
+
+def run_configs(args):
+    """Per configuration: FP64 and precision-form step time and the per-field
+    relative L2 difference of the two after the same steps (one JSON line each)."""
+    import numpy as np
+    import torch
+
+    import eulerianfsi_b200 as ef
+    torch.cuda.set_device(0)
+    for name, (make, steps) in CONFIGS.items():
+        res = {}
+        for prec in ("fp64", "mixed"):
+            w = make(prec)
+            ctx = ef.build_imex_context(w.metrics, w.bcs, w.models, numerics=w.numerics)
+            h = ctx.handle
+            st = w.state.copy()
+            h.upload(st)
+            h.set_correction(np.zeros((w.metrics.Nx, w.metrics.Ny), order="F"))
+            if w.needs_compatible_start:
+                ef.make_velocity_compatible(st, ctx, ef.allocate_imex_workspace(w.metrics))
+                h.upload(st)
+            dts = (C.c_double * steps)(*([w.dt] * steps))
+            h.call("step_n", 0.0, dts, steps, None)
+            ms = h.stats()["device_ms"] / steps
+            out = st.copy()
+            h.download(out)
+            res[prec] = (ms, out, w.cells)
+        errs = {f: float(np.linalg.norm(getattr(res["mixed"][1], f) - getattr(res["fp64"][1], f))
+                         / max(np.linalg.norm(getattr(res["fp64"][1], f)), 1e-300))
+                for f in ("U", "V", "phi", "resource", "sigma_xx", "sigma_yy", "sigma_xy")}
+        cells = res["fp64"][2]
+        print(json.dumps({"config": name, "steps": steps, "fp64_ms_per_step": res["fp64"][0],
+                          "mixed_ms_per_step": res["mixed"][0],
+                          "fp64_cell_steps_per_s": cells / (res["fp64"][0] / 1e3),
+                          "mixed_cell_steps_per_s": cells / (res["mixed"][0] / 1e3),
+                          "speedup": res["fp64"][0] / res["mixed"][0], "rel_l2_mixed_vs_fp64": errs}),
+              flush=True)
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -324,7 +375,12 @@ def main():
     p.add_argument("--reference-budget", type=float, default=150.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    p.add_argument("--configs", action="store_true",
+                   help="FP64 vs precision form on the four benchmark configurations (1 GPU)")
     args = p.parse_args()
+    if args.configs:
+        run_configs(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -498,3 +498,29 @@ def test_state_diagnostics_match_oracle(name):
 
     close(g, o, "diag")
     assert g["global_region"]["cells"] == w.metrics.Nx * w.metrics.Ny
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-8), ("mixed", 1e-6)])
+def test_config0_full_length_against_oracle(precision, tol):
+    """Config 0 (cavity with a deformable disk, 64 x 64, 200 steps) in both precision
+    forms against the FP64 oracle: every field within 1e-8 (FP64 step) or 1e-6
+    (precision form) relative L2 after the full run, solves converged to 1e-13."""
+    w = workloads.cavity_disk(N=64, precision=precision)
+    import dataclasses
+    ls = dataclasses.replace(w.numerics.linear_solvers, velocity_method="gmres", reltol=1e-13, maxiter=2000)
+    num = dataclasses.replace(w.numerics, linear_solvers=ls, projection_reltol=1e-13, projection_maxiter=3000)
+    gpu, ora = pair(w.metrics, w.bcs, w.models, num)
+    dts = (C.c_double * w.steps)(*([w.dt] * w.steps))
+    out = []
+    for h in (gpu, ora):
+        st = w.state.copy()
+        h.upload(st)
+        h.set_correction(fz(64, 64))
+        if h is gpu:
+            h.call("step_n", 0.0, dts, w.steps, None)
+        else:
+            for k in range(w.steps):
+                h.call("integrate_step", k * w.dt, w.dt, None)
+        h.download(st)
+        out.append(st)
+    _assert_states(out[0], out[1], tol)
