@@ -55,8 +55,8 @@ __global__ void __launch_bounds__(TX* TY) k_phase(Params P, const double* __rest
         int a = t % SX, b = t / SX;
         int gi = i0 - H + a, gj = j0 - H + b;
         bool valid = true;
-        if (px) gi = wrapi(gi, Nx); else valid &= (gi >= 0 && gi < Nx);
-        if (py) gj = wrapi(gj, Ny); else valid &= (gj >= 0 && gj < Ny);
+        if (px) gi = wrapm(gi, Nx); else valid &= (gi >= 0 && gi < Nx);
+        if (py) gj = wrapm(gj, Ny); else valid &= (gj >= 0 && gj < Ny);
         double p = valid ? phi[cidx(gi, gj, Nx)] : 0.0;
         s_phi[b][a] = p;
         if (METHOD == EFSI_PF_ACDI) {
@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(TX* TY) k_phase(Params P, const double* __rest
                 s_nx[b][a] = 0.0; s_ny[b][a] = 0.0;
                 continue;
             }
-            int ci = px ? wrapi(gi, Nx) : gi, cj = py ? wrapi(gj, Ny) : gj;
+            int ci = px ? wrapm(gi, Nx) : gi, cj = py ? wrapm(gj, Ny) : gj;
             const double(*F)[SX] = (METHOD == EFSI_PF_ACDI || smooth9) ? s_aux : s_phi;
             // face gradients of F at the four faces of the cell
             auto fgx = [&](bool right) -> double {
