@@ -354,6 +354,44 @@ def run_configs(args):
               flush=True)
 
 
+def run_sensitivity(args, rank, world, dist):
+    """Finite-difference sensitivities of the cavity-disk objective (N=256 to T=2 by
+    default): one ensemble of forward runs (base, +/- h per parameter, +/- h along a
+    seeded direction) spread over the ranks, and the FD gradient's cost in forward
+    runs.  Rank 0 prints one JSON line."""
+    import time
+
+    import torch
+
+    from eulerianfsi_b200 import sensitivity as sens
+    times = []
+    ev = sens.make_evaluator(args.sens_N, args.sens_T, timings=times)
+    group = dist.group.WORLD if dist else None
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    res = sens.gradient_check(ev, seed=args.sens_seed, group=group)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    dev_ms = float(sum(times))
+    if dist:
+        wall = max_over_ranks(wall, dist, "cuda")
+        dev_ms = max_over_ranks(dev_ms, dist, "cuda")
+    if rank:
+        return
+    forward_ms = times[0]  # run 0 (the base point) always runs on rank 0
+    steps = int(round(args.sens_T / (0.2 / args.sens_N)))
+    res.update({"config": {"workload": "cavity_disk_sensitivity", "Nx": args.sens_N, "Ny": args.sens_N,
+                           "T": args.sens_T, "steps": steps, "dt": 0.2 / args.sens_N, "precision": "fp64",
+                           "solver_reltol": sens.FD_RELTOL, "parameters": list(sens.PARAMETERS),
+                           "at": list(sens.DEFAULT_PARAMETERS), "seed": args.sens_seed, "rel_h": 1e-6},
+                "n_gpus": world, "method": "central differences (discrete adjoint not built)",
+                "forward_ms": forward_ms, "forward_cell_steps_per_s": args.sens_N ** 2 * steps / (forward_ms / 1e3),
+                "gradient_cost_in_forward_runs": 2 * len(sens.PARAMETERS),
+                "ensemble_device_ms_max_over_ranks": dev_ms, "ensemble_wall_s": wall})
+    print(json.dumps(res), flush=True)
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -377,6 +415,11 @@ def main():
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     p.add_argument("--configs", action="store_true",
                    help="FP64 vs precision form on the four benchmark configurations (1 GPU)")
+    p.add_argument("--sensitivity", action="store_true",
+                   help="finite-difference sensitivities of the cavity-disk objective, runs spread over ranks")
+    p.add_argument("--sens-N", type=int, default=256)
+    p.add_argument("--sens-T", type=float, default=2.0)
+    p.add_argument("--sens-seed", type=int, default=0)
     args = p.parse_args()
     if args.configs:
         run_configs(args)
@@ -392,6 +435,11 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank)
+        elif args.sensitivity:
+            import torch
+            torch.cuda.set_device(local_rank)
+            import torch.distributed as dist
+            run_sensitivity(args, rank, world, dist if world > 1 else None)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

@@ -8,6 +8,8 @@ the reference drivers), as (metrics, bcs, models, numerics, state, dt, steps).
                        (run_wall_supported_filament_kolmogorov_flow.jl:371-557)
   cavity_disks20       cavity physics with 20 seeded disks of radius 0.05, N=1024
   channel_growth       open channel [0,2]x[0,1], 1024x512, growth and resource
+  cavity_disk_sensitivity  cavity_disk at N=256 to T=2 with (G, lid speed, disk centre)
+                       as parameters, for the finite-difference sensitivities
 """
 from __future__ import annotations
 
@@ -56,8 +58,8 @@ def _numerics(projection_reltol, velocity_reltol, precision, extension=True):
                         projection_maxiter=3000, projection_restart=50, precision=precision, **kw)
 
 
-def _cavity_bcs():
-    wall, lid = Dirichlet(0.0), Dirichlet(1.0)
+def _cavity_bcs(lid_speed=1.0):
+    wall, lid = Dirichlet(0.0), Dirichlet(float(lid_speed))
     noflux = BoundaryConditionSetup(Neumann(0.0), Neumann(0.0), Neumann(0.0), Neumann(0.0))
     return FSIBoundaryConditions(
         BoundaryConditionSetup(wall, wall, wall, lid), BoundaryConditionSetup(wall, wall, wall, wall),
@@ -86,6 +88,23 @@ def cavity_disk(N=64, steps=200, projection_reltol=1e-10, velocity_reltol=1e-8, 
     modulus = 0.1
     dt = 0.2 * h / max(1.0, math.sqrt(modulus / 1.0))
     return Workload("cavity_disk", grid, metrics, _cavity_bcs(), _cavity_models(h, modulus),
+                    _numerics(projection_reltol, velocity_reltol, precision), _rest_state(N, N, phi),
+                    dt, steps)
+
+
+def cavity_disk_sensitivity(N=256, params=(0.1, 1.0, 0.6, 0.5), T=2.0, projection_reltol=1e-10,
+                            velocity_reltol=1e-8, precision="fp64"):
+    """The differentiation configuration: the cavity_disk physics with its shear
+    modulus G, lid speed and initial disk centre (x, y) taken from `params`, run to
+    time T at the fixed step dt = 0.2/N, so that perturbing G leaves dt alone."""
+    G, lid, cx, cy = (float(v) for v in params)
+    grid = generate_grid(1.0, 1.0, N, N)
+    metrics = build_mesh_metrics(grid)
+    h = 1.0 / N
+    phi = initialize_circle(grid, (cx, cy), 0.2, 1.5 * h)
+    dt = 0.2 * h
+    steps = int(round(T / dt))
+    return Workload("cavity_disk_sensitivity", grid, metrics, _cavity_bcs(lid), _cavity_models(h, G),
                     _numerics(projection_reltol, velocity_reltol, precision), _rest_state(N, N, phi),
                     dt, steps)
 

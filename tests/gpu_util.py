@@ -50,3 +50,20 @@ def call_both(gpu, ora, name, *args_factory):
         h.call(name, *args)
         outs.append(keep)
     return outs
+
+
+def oracle_final_state(w):
+    """Run workload `w` for w.steps oracle steps from its initial state; the final state."""
+    from tests.helpers import fz
+    h = Handle(load_oracle(), "oracle_", ConfigBlock(w.metrics, w.bcs, w.models, w.numerics), w.metrics)
+    state = w.state.copy()
+    h.upload(state)
+    h.set_correction(fz(w.metrics.Nx, w.metrics.Ny))
+    t = 0.0
+    for _ in range(w.steps):
+        rep = _abi.StepReportC()
+        h.call("integrate_step", t, w.dt, C.byref(rep))
+        t += w.dt
+    h.download(state)
+    h.close()
+    return state
