@@ -195,11 +195,28 @@ __device__ bool grid_reduce(double (&v)[NV], const RedSlot& rs, double (&tot)[NV
     __syncthreads();
     if (!last) return false;
     __threadfence();
+    // The last block reads nb x NV partials from L2.  Each round issues U x NV
+    // independent loads before the first add, so a thread waits about
+    // nb / (nthr * U) load latencies, not nb / nthr * NV of them.
+    constexpr int U = NV >= 8 ? 1 : (NV >= 4 ? 2 : 8 / NV);
     double acc[NV];
 #pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        acc[k] = MAXOP ? -1.0e308 : 0.0;
-        for (int b = tid; b < nb; b += nthr) {
+    for (int k = 0; k < NV; ++k) acc[k] = MAXOP ? -1.0e308 : 0.0;
+    int b = tid;
+    for (; b + (U - 1) * nthr < nb; b += U * nthr) {
+        double x[U][NV];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int k = 0; k < NV; ++k) x[u][k] = __ldcg(&rs.part[(size_t)k * rs.maxBlocks + b + u * nthr]);
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int k = 0; k < NV; ++k) acc[k] = MAXOP ? fmax(acc[k], x[u][k]) : acc[k] + x[u][k];
+    }
+    for (; b < nb; b += nthr) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
             double x = __ldcg(&rs.part[(size_t)k * rs.maxBlocks + b]);
             acc[k] = MAXOP ? fmax(acc[k], x) : acc[k] + x;
         }

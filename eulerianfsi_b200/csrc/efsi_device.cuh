@@ -67,4 +67,54 @@ __device__ __forceinline__ MuField make_mu(const Params& P, const double* phi) {
     return MuField{phi, P.md.viscosity, P.md.viscosity_fluid, P.md.viscosity_structure, P.g.Nx, P.g.Ny, P.g.px, P.g.py};
 }
 
+// Matrix part of the viscous operator (no boundary data), rows u(i,j) and v(i,j).
+// INT: (i,j) is at least one cell away from every edge, so no boundary branch is
+// taken (the same arithmetic as the general path there, without its tests).
+// Constant viscosity known to the compiler (the common case: ConstantViscosity).
+struct MuConst {
+    double m;
+    __device__ __forceinline__ double c(int, int) const { return m; }
+    __device__ __forceinline__ double k(int, int) const { return m; }
+};
+
+template <bool INT, class X, class MU>
+__device__ __forceinline__ void visc_A(const Params& P, const MU& mu, const X& x, int i, int j, double& au,
+                                       double& av) {
+    const int Nx = P.g.Nx, Ny = P.g.Ny;
+    const double ihx = P.g.ihx, ihy = P.g.ihy;
+    const bool px = P.g.px, py = P.g.py;
+    auto txx = [&](int c, int r) {
+        double nxt = (INT || c < Nx - 1) ? x.U(c + 1, r) : (px ? x.U(0, r) : 0.0);
+        return 2.0 * mu.c(c, r) * ((nxt - x.U(c, r)) * ihx);
+    };
+    auto tyy = [&](int c, int r) {
+        double nxt = (INT || r < Ny - 1) ? x.V(c, r + 1) : (py ? x.V(c, 0) : 0.0);
+        return 2.0 * mu.c(c, r) * ((nxt - x.V(c, r)) * ihy);
+    };
+    auto txy = [&](int c, int r) {
+        double duy = (INT || r > 0) ? (x.U(c, r) - x.U(c, r - 1)) * ihy
+                                    : (py ? (x.U(c, 0) - x.U(c, Ny - 1)) * ihy : 0.0);
+        double dvx = (INT || c > 0) ? (x.V(c, r) - x.V(c - 1, r)) * ihx
+                                    : (px ? (x.V(0, r) - x.V(Nx - 1, r)) * ihx : 0.0);
+        return 2.0 * mu.k(c, r) * (0.5 * duy + 0.5 * dvx);
+    };
+    double axx = txx(i, j) - ((INT || i > 0) ? txx(i - 1, j) : (px ? txx(Nx - 1, j) : 0.0));
+    double axy = -txy(i, j) + ((INT || j < Ny - 1) ? txy(i, j + 1) : (py ? txy(i, 0) : 0.0));
+    au = axx * ihx + axy * ihy;
+    double ayx = -txy(i, j) + ((INT || i < Nx - 1) ? txy(i + 1, j) : (px ? txy(0, j) : 0.0));
+    double ayy = tyy(i, j) - ((INT || j > 0) ? tyy(i, j - 1) : (py ? tyy(i, Ny - 1) : 0.0));
+    av = ayx * ihx + ayy * ihy;
+    if (INT) return;
+    if (!py) {
+        if (j == 0 && P.bu.s[BOTTOM].type == EFSI_BC_DIRICHLET) au -= mu.k(i, 0) / (P.g.hy * (0.5 * P.g.hy)) * x.U(i, 0);
+        if (j == Ny - 1 && P.bu.s[TOP].type == EFSI_BC_DIRICHLET)
+            au -= mu.k(i, Ny) / (P.g.hy * (0.5 * P.g.hy)) * x.U(i, Ny - 1);
+    }
+    if (!px) {
+        if (i == 0 && P.bv.s[LEFT].type == EFSI_BC_DIRICHLET) av -= mu.k(0, j) / (P.g.hx * (0.5 * P.g.hx)) * x.V(0, j);
+        if (i == Nx - 1 && P.bv.s[RIGHT].type == EFSI_BC_DIRICHLET)
+            av -= mu.k(Nx, j) / (P.g.hx * (0.5 * P.g.hx)) * x.V(Nx - 1, j);
+    }
+}
+
 }  // namespace efsi

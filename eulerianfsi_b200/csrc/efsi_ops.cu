@@ -623,11 +623,31 @@ void launch_capillary_curvature(const Params& P, const double* phi, double* smoo
 }
 
 // ---- compact viscous operator application (Operators.jl:929-1083, :1115) ------------------------
+// Full MAC arrays seen through the accessor interface of visc_A.
+struct MacUV {
+    const double* u;
+    const double* v;
+    int Nx;
+    __device__ __forceinline__ double U(int i, int j) const { return u[uidx(i, j, Nx)]; }
+    __device__ __forceinline__ double V(int i, int j) const { return v[vidx(i, j, Nx)]; }
+};
+
 __global__ void k_viscous_apply(Params P, const double* __restrict__ U, const double* __restrict__ V,
                                 const double* __restrict__ phi, double* Iu, double* Iv) {
     const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
     const int Nx = P.g.Nx, Ny = P.g.Ny;
     if (i >= Nx || j >= Ny) return;
+    if (i >= 1 && i <= Nx - 2 && j >= 1 && j <= Ny - 2) {
+        // interior: no boundary data enters; the same arithmetic as below without its tests
+        double au, av;
+        if (P.md.viscosity == EFSI_VISC_CONSTANT)
+            visc_A<true>(P, MuConst{P.md.viscosity_fluid}, MacUV{U, V, Nx}, i, j, au, av);
+        else
+            visc_A<true>(P, make_mu(P, phi), MacUV{U, V, Nx}, i, j, au, av);
+        Iu[cidx(i, j, Nx)] = au;
+        Iv[cidx(i, j, Nx)] = av;
+        return;
+    }
     MuField mu = make_mu(P, phi);
     const double ihx = P.g.ihx, ihy = P.g.ihy;
     auto u = [&](int a, int b) { return U[uidx(a, b, Nx)]; };

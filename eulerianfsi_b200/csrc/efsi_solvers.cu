@@ -30,6 +30,19 @@ namespace efsi {
 static constexpr int BX = 32, BY = 8;
 static inline dim3 grid2(int nx, int ny) { return dim3((nx + BX - 1) / BX, (ny + BY - 1) / BY); }
 
+// Persistent loop over the BX x BY tiles of an nx x ny index space (1-D grid of
+// BX x BY blocks); f(i, j) runs for the points inside it.  A kernel that ends in a
+// grid reduction accumulates over all its tiles and reduces once per block.
+template <class F>
+__device__ __forceinline__ void for_tiles(int nx, int ny, F&& f) {
+    const int ntx = (nx + BX - 1) / BX, nt = ntx * ((ny + BY - 1) / BY);
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int i = (t % ntx) * BX + threadIdx.x, j = (t / ntx) * BY + threadIdx.y;
+        if (i < nx && j < ny) f(i, j);
+    }
+}
+static inline int tiles2(int nx, int ny) { return ((nx + BX - 1) / BX) * ((ny + BY - 1) / BY); }
+
 // =====================================================================================
 // Viscous operator pieces
 // =====================================================================================
@@ -41,55 +54,6 @@ struct CompactUV {
     __device__ __forceinline__ double V(int i, int j) const { return v[cidx(i, j, Nx)]; }
 };
 
-// Matrix part of the viscous operator (no boundary data), rows u(i,j) and v(i,j).
-// INT: (i,j) is at least one cell away from every edge, so no boundary branch is
-// taken (the same arithmetic as the general path there, without its tests).
-// Constant viscosity known to the compiler (the common case: ConstantViscosity).
-struct MuConst {
-    double m;
-    __device__ __forceinline__ double c(int, int) const { return m; }
-    __device__ __forceinline__ double k(int, int) const { return m; }
-};
-
-template <bool INT, class X, class MU>
-__device__ __forceinline__ void visc_A(const Params& P, const MU& mu, const X& x, int i, int j, double& au,
-                                       double& av) {
-    const int Nx = P.g.Nx, Ny = P.g.Ny;
-    const double ihx = P.g.ihx, ihy = P.g.ihy;
-    const bool px = P.g.px, py = P.g.py;
-    auto txx = [&](int c, int r) {
-        double nxt = (INT || c < Nx - 1) ? x.U(c + 1, r) : (px ? x.U(0, r) : 0.0);
-        return 2.0 * mu.c(c, r) * ((nxt - x.U(c, r)) * ihx);
-    };
-    auto tyy = [&](int c, int r) {
-        double nxt = (INT || r < Ny - 1) ? x.V(c, r + 1) : (py ? x.V(c, 0) : 0.0);
-        return 2.0 * mu.c(c, r) * ((nxt - x.V(c, r)) * ihy);
-    };
-    auto txy = [&](int c, int r) {
-        double duy = (INT || r > 0) ? (x.U(c, r) - x.U(c, r - 1)) * ihy
-                                    : (py ? (x.U(c, 0) - x.U(c, Ny - 1)) * ihy : 0.0);
-        double dvx = (INT || c > 0) ? (x.V(c, r) - x.V(c - 1, r)) * ihx
-                                    : (px ? (x.V(0, r) - x.V(Nx - 1, r)) * ihx : 0.0);
-        return 2.0 * mu.k(c, r) * (0.5 * duy + 0.5 * dvx);
-    };
-    double axx = txx(i, j) - ((INT || i > 0) ? txx(i - 1, j) : (px ? txx(Nx - 1, j) : 0.0));
-    double axy = -txy(i, j) + ((INT || j < Ny - 1) ? txy(i, j + 1) : (py ? txy(i, 0) : 0.0));
-    au = axx * ihx + axy * ihy;
-    double ayx = -txy(i, j) + ((INT || i < Nx - 1) ? txy(i + 1, j) : (px ? txy(0, j) : 0.0));
-    double ayy = tyy(i, j) - ((INT || j > 0) ? tyy(i, j - 1) : (py ? tyy(i, Ny - 1) : 0.0));
-    av = ayx * ihx + ayy * ihy;
-    if (INT) return;
-    if (!py) {
-        if (j == 0 && P.bu.s[BOTTOM].type == EFSI_BC_DIRICHLET) au -= mu.k(i, 0) / (P.g.hy * (0.5 * P.g.hy)) * x.U(i, 0);
-        if (j == Ny - 1 && P.bu.s[TOP].type == EFSI_BC_DIRICHLET)
-            au -= mu.k(i, Ny) / (P.g.hy * (0.5 * P.g.hy)) * x.U(i, Ny - 1);
-    }
-    if (!px) {
-        if (i == 0 && P.bv.s[LEFT].type == EFSI_BC_DIRICHLET) av -= mu.k(0, j) / (P.g.hx * (0.5 * P.g.hx)) * x.V(0, j);
-        if (i == Nx - 1 && P.bv.s[RIGHT].type == EFSI_BC_DIRICHLET)
-            av -= mu.k(Nx, j) / (P.g.hx * (0.5 * P.g.hx)) * x.V(Nx - 1, j);
-    }
-}
 template <class X>
 __device__ __forceinline__ void visc_A_any(const Params& P, const MuField& mu, const X& x, int i, int j, double& au,
                                            double& av) {
@@ -144,11 +108,10 @@ __global__ void k_visc_init(Params P, DtCoef ac, double reltol, int maxiter, con
                             double* dinv_u, double* dinv_v, CGScal* cg, RedSlot rs, int* iters_out,
                             cudaGraphConditionalHandle cond) {
     __shared__ double sh[64];
-    const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
     const int Nx = P.g.Nx;
     const double alpha = ac.value();
     double acc[2] = {0.0, 0.0};
-    if (i < Nx && j < P.g.Ny) {
+    for_tiles(Nx, P.g.Ny, [&](int i, int j) {
         MuField mu = make_mu(P, phi);
         CompactUV x{xu, xv, Nx};
         double au, av, du, dv;
@@ -163,9 +126,9 @@ __global__ void k_visc_init(Params P, DtCoef ac, double reltol, int maxiter, con
         rv[k] = r2;
         dinv_u[k] = d1;
         dinv_v[k] = d2;
-        acc[0] = r1 * r1 + r2 * r2;
-        acc[1] = r1 * r1 * d1 + r2 * r2 * d2;
-    }
+        acc[0] += r1 * r1 + r2 * r2;
+        acc[1] += r1 * r1 * d1 + r2 * r2 * d2;
+    });
     double tot[2];
     if (grid_reduce<2>(acc, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0) {
         cg->rr0 = tot[0];
@@ -224,6 +187,32 @@ __device__ __forceinline__ void visc_halo_slot(int h, int& lx, int& ly) {
     else { int t = h - 2 * VSX; lx = t < VTY ? 0 : VSX - 1; ly = 1 + (t % VTY); }
 }
 
+// Shared-memory view of a tile that lies with its halo inside the grid: every
+// request is within one cell of the tile, so no request wraps.
+struct TileIn {
+    const double* su;
+    const double* sv;
+    int i0, j0;
+    __device__ __forceinline__ int slot(int c, int r) const { return (r - j0 + 1) * VSX + (c - i0 + 1); }
+    __device__ __forceinline__ double U(int c, int r) const { return su[slot(c, r)]; }
+    __device__ __forceinline__ double V(int c, int r) const { return sv[slot(c, r)]; }
+};
+
+// A tile (i0, j0) whose points and halo all lie at least one cell inside the edges:
+// no wrapped index, no Dirichlet row, no boundary term in its stencils.
+__device__ __forceinline__ bool visc_tile_inside(int i0, int j0, int Nx, int Ny) {
+    return i0 >= 1 && j0 >= 1 && i0 + VTX <= Nx - 1 && j0 + VTY <= Ny - 1;
+}
+
+// A u at an interior point of an inside tile (the interior form of visc_A_tile).
+__device__ __forceinline__ void visc_A_inside(const Params& P, const double* phi, const TileIn& t, int i, int j,
+                                              double& au, double& av) {
+    if (P.md.viscosity == EFSI_VISC_CONSTANT)
+        visc_A<true>(P, MuConst{P.md.viscosity_fluid}, t, i, j, au, av);
+    else
+        visc_A<true>(P, make_mu(P, phi), t, i, j, au, av);
+}
+
 // A u at (i,j) from a staged tile; interior points of a constant-viscosity model take
 // the specialised form (same arithmetic, viscosity known to the compiler).
 __device__ __forceinline__ void visc_A_tile(const Params& P, const double* phi, const TileUV& t, int i, int j,
@@ -266,6 +255,18 @@ __device__ __forceinline__ void visc_stage_value(const Params& P, const ViscIter
         hu = d1 * (r1 - a * s1);
         hv = d2 * (r2 - a * s2);
     }
+}
+
+// visc_stage_value<false> at a slot of an inside tile (no wrap, no wall).
+__device__ __forceinline__ void visc_stage_inside(const ViscIterArgs& v, bool first, double a, double b, size_t k,
+                                                  double& hu, double& hv) {
+    const double d1 = __ldg(v.dinv_u + k), d2 = __ldg(v.dinv_v + k);
+    const double r1 = __ldg(v.r_u + k), r2 = __ldg(v.r_v + k);
+    const double w1 = __ldg(v.w_u + k), w2 = __ldg(v.w_v + k);
+    const double s1 = first ? w1 : w1 + b * __ldg(v.s_u + k);
+    const double s2 = first ? w2 : w2 + b * __ldg(v.s_v + k);
+    hu = d1 * (r1 - a * s1);
+    hv = d2 * (r2 - a * s2);
 }
 
 // w_0 = A M r_0 and d_0 = u_0.w_0 -> a_0 = g_0 / d_0.
@@ -344,12 +345,14 @@ __global__ void __launch_bounds__(VTX * VTY, 4) k_visc_cg(Params P, DtCoef ac, c
             }
             x1 = v.x_u[k]; x2 = v.x_v[k];
         }
+        const bool inside = visc_tile_inside(i0, j0, Nx, Ny);
         const bool halo = tid < 2 * VSX + 2 * VTY;
         int hx = 0, hy = 0;
         double hu = 0.0, hv = 0.0;
         if (halo) {
             visc_halo_slot(tid, hx, hy);
-            visc_stage_value<false>(P, v, first, a, b, i0 + hx - 1, j0 + hy - 1, hu, hv);
+            if (inside) visc_stage_inside(v, first, a, b, cidx(i0 + hx - 1, j0 + hy - 1, Nx), hu, hv);
+            else visc_stage_value<false>(P, v, first, a, b, i0 + hx - 1, j0 + hy - 1, hu, hv);
         }
         double un = 0.0, vn = 0.0;
         if (own) {
@@ -381,9 +384,15 @@ __global__ void __launch_bounds__(VTX * VTY, 4) k_visc_cg(Params P, DtCoef ac, c
         }
         __syncthreads();
         if (own) {
-            TileUV tl{su, sv, i0, j0, Nx, Ny};
             double w1, w2;
-            visc_apply_tile(P, alpha, phi, tl, i, j, un, vn, w1, w2);
+            if (inside) {
+                double au, av;
+                visc_A_inside(P, phi, TileIn{su, sv, i0, j0}, i, j, au, av);
+                w1 = un - alpha * au;
+                w2 = vn - alpha * av;
+            } else {
+                visc_apply_tile(P, alpha, phi, TileUV{su, sv, i0, j0, Nx, Ny}, i, j, un, vn, w1, w2);
+            }
             const size_t k = cidx(i, j, Nx);
             v.wn_u[k] = w1;
             v.wn_v[k] = w2;
@@ -422,7 +431,7 @@ void visc_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const 
                cudaStream_t s) {
     dim3 g = grid2(P.g.Nx, P.g.Ny), b(BX, BY);
     k_visc_x0<<<g, b, 0, s>>>(P, Un, Vn, w.x_u, w.x_v);
-    k_visc_init<<<g, b, 0, s>>>(P, alpha, reltol, maxiter, w.x_u, w.x_v, rhs_u, rhs_v, phi, w.r_u[0], w.r_v[0],
+    k_visc_init<<<persistent_grid(tiles2(P.g.Nx, P.g.Ny), P.nsm, 2), b, 0, s>>>(P, alpha, reltol, maxiter, w.x_u, w.x_v, rhs_u, rhs_v, phi, w.r_u[0], w.r_v[0],
                                 w.dinv_u, w.dinv_v, cg, rs, iters_out, cond);
     // w_0 goes to the parity-0 "read" slot: the first iteration reads (r, w)[0].
     ViscIterArgs v = visc_args(w, 1);
@@ -457,14 +466,21 @@ struct ViscMxArgs {
 
 // FP64 value staged at tile slot (gi, gj): x (REFINE/START), M rR (RESTART) or
 // M (r_i - a (w_i + b s_{i-1})) (ITER); zero outside walls, wrapped when periodic.
+// `inside`: the slot is known to lie in the grid (a halo slot of an inside tile).
 __device__ __forceinline__ void visc_mx_slot(const Params& P, const ViscMxArgs& v, int phase, bool first, double a,
-                                             double b, int gi, int gj, double& hu, double& hv) {
+                                             double b, int gi, int gj, double& hu, double& hv,
+                                             bool inside = false) {
     const int Nx = P.g.Nx, Ny = P.g.Ny;
-    const bool inx = gi >= 0 && gi < Nx, iny = gj >= 0 && gj < Ny;
-    hu = 0.0;
-    hv = 0.0;
-    if (!((inx || P.g.px) && (iny || P.g.py))) return;
-    const size_t k = cidx(inx ? gi : wrapm(gi, Nx), iny ? gj : wrapm(gj, Ny), Nx);
+    size_t k;
+    if (inside) {
+        k = cidx(gi, gj, Nx);
+    } else {
+        const bool inx = gi >= 0 && gi < Nx, iny = gj >= 0 && gj < Ny;
+        hu = 0.0;
+        hv = 0.0;
+        if (!((inx || P.g.px) && (iny || P.g.py))) return;
+        k = cidx(inx ? gi : wrapm(gi, Nx), iny ? gj : wrapm(gj, Ny), Nx);
+    }
     if (phase == MX_REFINE) {
         hu = v.x_u[k];
         hv = v.x_v[k];
@@ -536,16 +552,38 @@ __global__ void __launch_bounds__(VTX * VTY, 3) k_visc_mx(Params P, DtCoef ac, d
         }
         su[(ty + 1) * VSX + tx + 1] = un;
         sv[(ty + 1) * VSX + tx + 1] = vn;
+        const bool inside = !START && visc_tile_inside(i0, j0, Nx, Ny);
         if (tid < 2 * VSX + 2 * VTY) {
             int lx, ly;
             visc_halo_slot(tid, lx, ly);
             double hu, hv;
-            visc_mx_slot(P, v, phase, first, a, b, i0 + lx - 1, j0 + ly - 1, hu, hv);
+            visc_mx_slot(P, v, phase, first, a, b, i0 + lx - 1, j0 + ly - 1, hu, hv, inside);
             su[ly * VSX + lx] = hu;
             sv[ly * VSX + lx] = hv;
         }
         __syncthreads();
-        if (own) {
+        if (own && inside) {  // no Dirichlet row, no wrap (START never takes this path)
+            double au, av;
+            visc_A_inside(P, phi, TileIn{su, sv, i0, j0}, i, j, au, av);
+            if (phase == MX_REFINE) {
+                const double r1 = v.rhs_u[k] - (un - alpha * au);
+                const double r2 = v.rhs_v[k] - (vn - alpha * av);
+                v.rR_u[k] = (float)r1;
+                v.rR_v[k] = (float)r2;
+                acc[0] += r1 * r1 + r2 * r2;
+            } else {
+                const double w1 = un - alpha * au, w2 = vn - alpha * av;
+                v.wn_u[k] = (float)w1;
+                v.wn_v[k] = (float)w2;
+                acc[1] += un * w1 + vn * w2;
+                if (phase == MX_RESTART) {
+                    const double r1 = v.rR_u[k], r2 = v.rR_v[k];
+                    v.rn_u[k] = (float)r1;
+                    v.rn_v[k] = (float)r2;
+                    acc[0] += r1 * un + r2 * vn;
+                }
+            }
+        } else if (own) {
             TileUV tl{su, sv, i0, j0, Nx, Ny};
             MuField mu = make_mu(P, phi);
             double au, av;
@@ -1353,13 +1391,13 @@ struct PredIn {
 __global__ void k_proj_rhs(Params P, PredIn in, const double* __restrict__ G, double* Up, double* Vp, double* rhs,
                            double* bw, int nullspace, ProjScal* ps, RedSlot rs, DevStatus* st) {
     __shared__ double sh[32 * 6];
-    const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
     const int Nx = P.g.Nx, Ny = P.g.Ny;
     const double area = P.g.hx * P.g.hy;
-    if (j < Ny && i <= Nx) Up[uidx(i, j, Nx)] = in.U(P, i, j);
-    if (i < Nx && j <= Ny) Vp[vidx(i, j, Nx)] = in.V(P, i, j);
     double acc[6] = {0, 0, 0, 0, 0, 0};
-    if (i < Nx && j < Ny) {
+    for_tiles(Nx + 1, Ny + 1, [&](int i, int j) {
+        if (j < Ny) Up[uidx(i, j, Nx)] = in.U(P, i, j);
+        if (i < Nx) Vp[vidx(i, j, Nx)] = in.V(P, i, j);
+        if (i >= Nx || j >= Ny) return;
         double div = (in.U(P, i + 1, j) - in.U(P, i, j)) * P.g.ihx + (in.V(P, i, j + 1) - in.V(P, i, j)) * P.g.ihy;
         double g = G ? G[cidx(i, j, Nx)] : 0.0;
         double rr = (div - g) - q_boundary_vec(P, i, j);
@@ -1367,13 +1405,13 @@ __global__ void k_proj_rhs(Params P, PredIn in, const double* __restrict__ G, do
         rhs[k] = rr;
         double b = -rr * area;
         bw[k] = b;
-        acc[0] = rr * area;
-        acc[1] = fabs(rr) * area;
-        acc[2] = b;
-        acc[3] = rr * rr;
-        acc[4] = div * div * area;
-        acc[5] = g * g * area;
-    }
+        acc[0] += rr * area;
+        acc[1] += fabs(rr) * area;
+        acc[2] += b;
+        acc[3] += rr * rr;
+        acc[4] += div * div * area;
+        acc[5] += g * g * area;
+    });
     double tot[6];
     if (grid_reduce<6>(acc, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0) {
         for (int k = 0; k < 6; ++k) ps->v[k] = tot[k];
@@ -1388,7 +1426,7 @@ __global__ void k_proj_rhs(Params P, PredIn in, const double* __restrict__ G, do
 void proj_rhs(const Params& P, const Projection& pj, bool compact_in, const double* u_in, const double* v_in,
               const double* G, ProjScal* ps, const RedSlot& rs, DevStatus* st, cudaStream_t s) {
     PredIn in{u_in, v_in, compact_in ? 1 : 0};
-    k_proj_rhs<<<grid2(P.g.Nx + 1, P.g.Ny + 1), dim3(BX, BY), 0, s>>>(P, in, G, pj.Up, pj.Vp, pj.rhs, pj.b,
+    k_proj_rhs<<<persistent_grid(tiles2(P.g.Nx + 1, P.g.Ny + 1), P.nsm, 3), dim3(BX, BY), 0, s>>>(P, in, G, pj.Up, pj.Vp, pj.rhs, pj.b,
                                                                      pj.nullspace ? 1 : 0, ps, rs, st);
 }
 
@@ -1397,11 +1435,10 @@ __global__ void k_pcg_init(MGLevel L, int px, int py, double reltol, int maxiter
                            const double* __restrict__ b, double* x, double* r, const ProjScal* ps, CGScal* cg,
                            RedSlot rs, const DevStatus* st, int* iters_out, cudaGraphConditionalHandle cond) {
     __shared__ double sh[32];
-    const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
     const int nx = L.nx;
     const double bmean = ps->v[10];
     double acc[1] = {0.0};
-    if (i < L.nx && j < L.ny) {
+    for_tiles(L.nx, L.ny, [&](int i, int j) {
         double d;
         lev_diag(L, px, py, i, j, d);
         auto xf = [&](int a, int c) { return q0[cidx(a, c, nx)]; };
@@ -1409,8 +1446,8 @@ __global__ void k_pcg_init(MGLevel L, int px, int py, double reltol, int maxiter
         double rr = (b[k] - bmean) - (d * q0[k] - lev_off(L, px, py, i, j, xf));
         x[k] = q0[k];
         r[k] = rr;
-        acc[0] = rr * rr;
-    }
+        acc[0] += rr * rr;
+    });
     double tot[1];
     if (grid_reduce<1>(acc, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0) {
         cg->rr0 = tot[0]; cg->rr = tot[0];
@@ -1498,7 +1535,7 @@ void proj_cg_init(const Params& P, const Projection& pj, double reltol, int maxi
                   const ProjScal* ps, const RedSlot& rs, const RedSlot& rs2, const DevStatus* st, int* iters_out,
                   cudaGraphConditionalHandle cond, cudaStream_t s) {
     const MGLevel& L = pj.lev[0];
-    k_pcg_init<<<grid2(L.nx, L.ny), dim3(BX, BY), 0, s>>>(L, P.g.px, P.g.py, reltol, maxiter, q0, pj.b, pj.x,
+    k_pcg_init<<<persistent_grid(tiles2(L.nx, L.ny), P.nsm, 6), dim3(BX, BY), 0, s>>>(L, P.g.px, P.g.py, reltol, maxiter, q0, pj.b, pj.x,
                                                           pj.r[0], ps, cg, rs, st, iters_out, cond);
     vcycle(pj, pj.r[0], nullptr, cg, rs, rs2, nullptr, 0, P.g.px, P.g.py, s);
 }
@@ -1529,9 +1566,8 @@ void proj_update_vcycle(const Params& P, const Projection& pj, int parity, CGSca
 // ---- correction and diagnostics (Projection.jl:253-306) ---------------------------------------
 __global__ void k_proj_mean(MGLevel L, const double* __restrict__ x, ProjScal* ps, RedSlot rs, int nullspace) {
     __shared__ double sh[32];
-    const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
     double acc[1] = {0.0};
-    if (i < L.nx && j < L.ny) acc[0] = x[cidx(i, j, L.nx)];
+    for_tiles(L.nx, L.ny, [&](int i, int j) { acc[0] += x[cidx(i, j, L.nx)]; });
     double tot[1];
     if (grid_reduce<1>(acc, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0)
         ps->v[6] = nullspace ? tot[0] / ((double)L.nx * L.ny) : 0.0;
@@ -1577,12 +1613,11 @@ __global__ void k_proj_correct(Params P, MGLevel L, const double* __restrict__ x
                                const double* __restrict__ rhs, double* q_out, double* U_out, double* V_out,
                                ProjScal* ps, double* stage_linf, RedSlot rmax, RedSlot rsum, DevStatus* st) {
     __shared__ double sh[64];
-    const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
     const int Nx = P.g.Nx, Ny = P.g.Ny;
     const double mean = ps->v[6];
     const double area = P.g.hx * P.g.hy;
     double mx[1] = {0.0}, sm[2] = {0.0, 0.0};
-    if (i < Nx && j < Ny) {
+    for_tiles(Nx, Ny, [&](int i, int j) {
         size_t k = cidx(i, j, Nx);
         double uL = Up[uidx(i, j, Nx)] - q_grad_x(P, x, mean, i, j);
         double uR = Up[uidx(i + 1, j, Nx)] - q_grad_x(P, x, mean, i + 1, j);
@@ -1595,16 +1630,16 @@ __global__ void k_proj_correct(Params P, MGLevel L, const double* __restrict__ x
         q_out[k] = x[k] - mean;
         double g = G ? G[k] : 0.0;
         double c = ((uR - uL) * P.g.ihx + (vT - vB) * P.g.ihy) - g;
-        mx[0] = fabs(c);
-        sm[0] = c * c * area;
+        mx[0] = fmax(mx[0], fabs(c));
+        sm[0] += c * c * area;
         // linear residual of the unpinned operator: L q - rhs, L q = -(K x)/area
         double d;
         lev_diag(L, P.g.px, P.g.py, i, j, d);
         auto xf = [&](int a, int b) { return x[cidx(a, b, Nx)] - mean; };
         double Lq = -(d * (x[k] - mean) - lev_off(L, P.g.px, P.g.py, i, j, xf)) / area;
         double lr = Lq - rhs[k];
-        sm[1] = lr * lr;
-    }
+        sm[1] += lr * lr;
+    });
     double t1[1], t2[2];
     bool last1 = grid_reduce<1, true>(mx, rmax, t1, sh);
     if (last1 && threadIdx.x == 0 && threadIdx.y == 0) {
@@ -1627,9 +1662,10 @@ void proj_finish(const Params& P, const Projection& pj, const double* G, double*
                  ProjScal* ps, double* stage_linf, const RedSlot& rs1, const RedSlot& rs2, DevStatus* st,
                  cudaStream_t s) {
     const MGLevel& L = pj.lev[0];
-    dim3 g = grid2(L.nx, L.ny), b(BX, BY);
-    k_proj_mean<<<g, b, 0, s>>>(L, pj.x, ps, rs1, pj.nullspace ? 1 : 0);
-    k_proj_correct<<<g, b, 0, s>>>(P, L, pj.x, pj.Up, pj.Vp, G, pj.rhs, q_out, U_out, V_out, ps, stage_linf, rs1,
+    const int nt = tiles2(L.nx, L.ny);
+    dim3 b(BX, BY);
+    k_proj_mean<<<persistent_grid(nt, P.nsm, 8), b, 0, s>>>(L, pj.x, ps, rs1, pj.nullspace ? 1 : 0);
+    k_proj_correct<<<persistent_grid(nt, P.nsm, 3), b, 0, s>>>(P, L, pj.x, pj.Up, pj.Vp, G, pj.rhs, q_out, U_out, V_out, ps, stage_linf, rs1,
                                    rs2, st);
 }
 
