@@ -56,8 +56,11 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """Clock and throttle-reason sampling during the timed region: NVML polled every
+    5 ms from a thread of this process (nvidia-smi -lms 200 when NVML is missing).
+    Sampling only reads the GPU's state."""
 
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -65,9 +68,43 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []  # (sm_mhz, reason names) from NVML
+        self.max_mhz = 0.0
+        self.stop = threading.Event()
+
+    def _open_nvml(self):
+        import pynvml as nv
+        nv.nvmlInit()
+        visible = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v for v in visible.split(",") if v.strip()]
+        idx = int(ids[self.gpu]) if ids and ids[self.gpu].strip().isdigit() else self.gpu
+        h = nv.nvmlDeviceGetHandleByIndex(idx)
+        self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+        return nv, h, bits
+
+    def _poll(self, nv, h, bits):
+        while not self.stop.is_set():
+            try:
+                clk = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((clk, tuple(n for n, b in zip(self.NAMES, bits) if r & b)))
+            except Exception:
+                pass
+            self.stop.wait(0.005)
 
     def __enter__(self):
+        try:
+            nv, h, bits = self._open_nvml()
+            self.nvml = nv
+            self.thread = threading.Thread(target=self._poll, args=(nv, h, bits), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
@@ -83,6 +120,13 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        if self.nvml is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -91,8 +135,10 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], self.max_mhz, set()
+        for clk, names in self.samples:
+            sm.append(clk)
+            reasons.update(names)
         for line in self.lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
@@ -103,12 +149,13 @@ class ClockSampler:
             except ValueError:
                 continue
             sm.append(clk)
-            for name, val in zip(names, parts[5:9]):
+            for name, val in zip(self.NAMES, parts[5:9]):
                 if val.lower().startswith("active"):
                     reasons.add(name)
         busy = [s for s in sm if s > 600] or sm
         return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": mx or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml, 5 ms" if self.samples else "nvidia-smi, 200 ms"}
 
 
 def max_over_ranks(value: float, dist, device: str) -> float:

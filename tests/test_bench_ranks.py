@@ -51,3 +51,12 @@ def test_reference_arm_runs_on_rank_zero_only(capsys):
             raise AssertionError(name)
     bench.run_reference(A(), rank=1)
     assert capsys.readouterr().out == ""
+
+
+def test_clock_summary_reports_median_under_load_and_reasons():
+    s = bench.ClockSampler(0)
+    s.max_mhz = 1965.0
+    s.samples = [(345.0, ()), (1965.0, ()), (1950.0, ("sw_power_cap",)), (1965.0, ())]
+    out = s.summary()
+    assert out["sm_mhz"] == 1965.0 and out["sm_max_mhz"] == 1965.0
+    assert out["reasons"] == ["sw_power_cap"] and out["samples"] == 4
