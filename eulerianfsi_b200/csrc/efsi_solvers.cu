@@ -21,6 +21,7 @@
 // is set, so iterations can be enqueued without host round trips.
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "efsi_device.cuh"
 #include "efsi_solvers.cuh"
@@ -1231,8 +1232,32 @@ __global__ void k_mg_dense(int n, const S* __restrict__ Minv, const S* __restric
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row = blockIdx.x * 8 + warp;
     if (row < n) {
-        double s = 0.0;
-        for (int k = lane; k < n; k += 32) s += Minv[(size_t)row * n + k] * sb[k];
+        // 16-byte loads, eight per lane in flight before the adds (two accumulators);
+        // the row start is 16-byte aligned when n is a multiple of the vector width
+        const S* m = Minv + (size_t)row * n;
+        constexpr int VW = 16 / (int)sizeof(S);
+        double s0 = 0.0, s1 = 0.0;
+        if (n % VW == 0) {
+            using Vec = typename std::conditional<sizeof(S) == 4, float4, double2>::type;
+            const Vec* mv = reinterpret_cast<const Vec*>(m);
+            const int nv = n / VW;
+#pragma unroll 8
+            for (int q = lane; q < nv; q += 32) {
+                const Vec w = __ldg(mv + q);
+                const double* bb = sb + q * VW;
+                if constexpr (sizeof(S) == 4) {
+                    s0 += (double)w.x * bb[0] + (double)w.y * bb[1];
+                    s1 += (double)w.z * bb[2] + (double)w.w * bb[3];
+                } else {
+                    s0 += w.x * bb[0];
+                    s1 += w.y * bb[1];
+                }
+            }
+        } else {
+#pragma unroll 8
+            for (int k = lane; k < n; k += 32) s0 += (double)__ldg(m + k) * sb[k];
+        }
+        double s = s0 + s1;
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
         if (lane == 0) x[row] = (S)s;
     }
