@@ -525,6 +525,54 @@ __device__ __forceinline__ double body_y(const Params& P) {
     return P.md.body_force == EFSI_FORCE_CONSTANT ? P.md.body_force_param[1] : 0.0;
 }
 
+// Interior forms of conv_x/conv_y/ssd_x/ssd_y for 1 <= i <= Nx-2, 1 <= j <= Ny-2: the
+// branches the general helpers take at such faces whatever the periodicity, with the
+// same arithmetic, so no boundary test is left in the inlined code.
+__device__ __forceinline__ double conv_x_in(const Params& P, const double* U, const double* V, const double* G, int i,
+                                           int j) {
+    const int Nx = P.g.Nx;
+    auto u2 = [&](int c) {
+        double uc = 0.5 * U[uidx(c, j, Nx)] + 0.5 * U[uidx(c + 1, j, Nx)];
+        return uc * uc;
+    };
+    auto uc = [&](int jc) { return 0.5 * (U[uidx(i, jc - 1, Nx)] + U[uidx(i, jc, Nx)]); };
+    auto vc = [&](int jj) { return 0.5 * (V[vidx(i - 1, jj, Nx)] + V[vidx(i, jj, Nx)]); };
+    double cu = (u2(i) - u2(i - 1)) * P.g.ihx + (uc(j + 1) * vc(j + 1) - uc(j) * vc(j)) * P.g.ihy;
+    if (G) {
+        double Sx = 0.5 * G[cidx(i - 1, j, Nx)] + 0.5 * G[cidx(i, j, Nx)];
+        cu -= Sx * U[uidx(i, j, Nx)];
+    }
+    return cu;
+}
+__device__ __forceinline__ double conv_y_in(const Params& P, const double* U, const double* V, const double* G, int i,
+                                           int j) {
+    const int Nx = P.g.Nx;
+    auto v2 = [&](int c) {
+        double vc = 0.5 * V[vidx(i, c, Nx)] + 0.5 * V[vidx(i, c + 1, Nx)];
+        return vc * vc;
+    };
+    auto uc = [&](int ii) { return 0.5 * (U[uidx(ii, j - 1, Nx)] + U[uidx(ii, j, Nx)]); };
+    auto vc = [&](int ic) { return 0.5 * (V[vidx(ic - 1, j, Nx)] + V[vidx(ic, j, Nx)]); };
+    double cv = (uc(i + 1) * vc(i + 1) - uc(i) * vc(i)) * P.g.ihx + (v2(j) - v2(j - 1)) * P.g.ihy;
+    if (G) {
+        double Sy = 0.5 * G[cidx(i, j - 1, Nx)] + 0.5 * G[cidx(i, j, Nx)];
+        cv -= Sy * V[vidx(i, j, Nx)];
+    }
+    return cv;
+}
+__device__ __forceinline__ double ssd_x_in(const Params& P, const Cells& f, int i, int j) {
+    auto xface = [&](int r) { return 0.5 * (cell_txy(P, f, i - 1, r) + cell_txy(P, f, i, r)); };
+    double dxx = (cell_txx(P, f, i, j) - cell_txx(P, f, i - 1, j)) * P.g.ihx;
+    double dxy = (xface(j + 1) - xface(j - 1)) / (2.0 * P.g.hy);
+    return dxx + dxy;
+}
+__device__ __forceinline__ double ssd_y_in(const Params& P, const Cells& f, int i, int j) {
+    auto yface = [&](int c) { return 0.5 * (cell_txy(P, f, c, j - 1) + cell_txy(P, f, c, j)); };
+    double dyy = (cell_tyy(P, f, i, j) - cell_tyy(P, f, i, j - 1)) * P.g.ihy;
+    double dxy = (yface(i + 1) - yface(i - 1)) / (2.0 * P.g.hx);
+    return dyy + dxy;
+}
+
 template <bool FULL>
 __global__ void k_momentum(Params P, double t, const double* __restrict__ U, const double* __restrict__ V,
                            Cells cells, const double* __restrict__ G, const double* __restrict__ kappa,
@@ -533,6 +581,21 @@ __global__ void k_momentum(Params P, double t, const double* __restrict__ U, con
     const int Nx = P.g.Nx, Ny = P.g.Ny;
     const bool elastic = P.md.elastic_stress != EFSI_ELASTIC_NONE ||
                          (P.md.viscosity != EFSI_VISC_NONE && G != nullptr);
+    if (i >= 1 && i <= Nx - 2 && j >= 1 && j <= Ny - 2) {
+        double fx = -conv_x_in(P, U, V, G, i, j) + body_x(P, t, j);
+        double fy = -conv_y_in(P, U, V, G, i, j) + body_y(P);
+        if (kappa) {
+            fx += P.md.capillary_coefficient * c2fx(P, kappa, i, j) * sgrad_x(P, P.bphi, cells.phi, i, j);
+            fy += P.md.capillary_coefficient * c2fy(P, kappa, i, j) * sgrad_y(P, P.bphi, cells.phi, i, j);
+        }
+        if (elastic) {
+            fx += ssd_x_in(P, cells, i, j);
+            fy += ssd_y_in(P, cells, i, j);
+        }
+        Fx[FULL ? uidx(i, j, Nx) : cidx(i, j, Nx)] = fx;
+        Fy[FULL ? vidx(i, j, Nx) : cidx(i, j, Nx)] = fy;
+        return;
+    }
     // x-momentum at U face (i, j)
     if (j < Ny && (FULL ? i <= Nx : i < Nx)) {
         double fx = -conv_x(P, U, V, G, i, j) + body_x(P, t, j);
@@ -793,31 +856,51 @@ __global__ void k_structure(Params P, const double* __restrict__ U, const double
     if (i >= Nx || j >= Ny) return;
     const size_t k = cidx(i, j, Nx);
     const double ihx = P.g.ihx, ihy = P.g.ihy;
-    double ax = upwind_rhs<false>(P, P.bsxx, U, V, sxx, i, j, st, 4);
-    double ay = upwind_rhs<false>(P, P.bsyy, U, V, syy, i, j, st, 5);
-    double ac = upwind_rhs<false>(P, P.bsxy, U, V, sxy, i, j, st, 6);
-    double dudx = (U[uidx(i + 1, j, Nx)] - U[uidx(i, j, Nx)]) * ihx;
-    double dvdy = (V[vidx(i, j + 1, Nx)] - V[vidx(i, j, Nx)]) * ihy;
-    double divv = dudx + dvdy;
     auto Uc = [&](int r) { return 0.5 * U[uidx(i, r, Nx)] + 0.5 * U[uidx(i + 1, r, Nx)]; };
     auto Vc = [&](int c) { return 0.5 * V[vidx(c, j, Nx)] + 0.5 * V[vidx(c, j + 1, Nx)]; };
-    double dudy, dvdx;  // Operators.jl:474-583
-    if (P.g.py) dudy = (Uc(wrapi(j + 1, Ny)) - Uc(wrapi(j - 1, Ny))) / (2.0 * P.g.hy);
-    else if (j == 0) {
-        const SideD& s = P.bu.s[BOTTOM];
-        dudy = s.type == EFSI_BC_DIRICHLET ? (Uc(0) - wall_u_at_xc(s, i)) / (0.5 * P.g.hy) : -wall_u_at_xc(s, i);
-    } else if (j == Ny - 1) {
-        const SideD& s = P.bu.s[TOP];
-        dudy = s.type == EFSI_BC_DIRICHLET ? (wall_u_at_xc(s, i) - Uc(Ny - 1)) / (0.5 * P.g.hy) : wall_u_at_xc(s, i);
-    } else dudy = (Uc(j + 1) - Uc(j - 1)) / (2.0 * P.g.hy);
-    if (P.g.px) dvdx = (Vc(wrapi(i + 1, Nx)) - Vc(wrapi(i - 1, Nx))) / (2.0 * P.g.hx);
-    else if (i == 0) {
-        const SideD& s = P.bv.s[LEFT];
-        dvdx = s.type == EFSI_BC_DIRICHLET ? (Vc(0) - wall_u_at_xc(s, j)) / (0.5 * P.g.hx) : -wall_u_at_xc(s, j);
-    } else if (i == Nx - 1) {
-        const SideD& s = P.bv.s[RIGHT];
-        dvdx = s.type == EFSI_BC_DIRICHLET ? (wall_u_at_xc(s, j) - Vc(Nx - 1)) / (0.5 * P.g.hx) : wall_u_at_xc(s, j);
-    } else dvdx = (Vc(i + 1) - Vc(i - 1)) / (2.0 * P.g.hx);
+    double ax, ay, ac, dudy, dvdx;  // Operators.jl:474-583
+    if (i >= 1 && i <= Nx - 2 && j >= 1 && j <= Ny - 2) {
+        // interior: the branches upwind_rhs and the gradients below take here, whatever
+        // the periodicity (same arithmetic), with the face velocities loaded once
+        const double ul = U[uidx(i, j, Nx)], ur = U[uidx(i + 1, j, Nx)];
+        const double vb = V[vidx(i, j, Nx)], vt = V[vidx(i, j + 1, Nx)];
+        auto up = [&](const double* q) {
+            auto c = [&](int a, int b) { return q[cidx(a, b, Nx)]; };
+            const double fxr = ur * (ur >= 0.0 ? c(i, j) : c(i + 1, j));
+            const double fxl = ul * (ul >= 0.0 ? c(i - 1, j) : c(i, j));
+            const double fyt = vt * (vt >= 0.0 ? c(i, j) : c(i, j + 1));
+            const double fyb = vb * (vb >= 0.0 ? c(i, j - 1) : c(i, j));
+            return -((fxr - fxl) * ihx + (fyt - fyb) * ihy);
+        };
+        ax = up(sxx);
+        ay = up(syy);
+        ac = up(sxy);
+        dudy = (Uc(j + 1) - Uc(j - 1)) / (2.0 * P.g.hy);
+        dvdx = (Vc(i + 1) - Vc(i - 1)) / (2.0 * P.g.hx);
+    } else {
+        ax = upwind_rhs<false>(P, P.bsxx, U, V, sxx, i, j, st, 4);
+        ay = upwind_rhs<false>(P, P.bsyy, U, V, syy, i, j, st, 5);
+        ac = upwind_rhs<false>(P, P.bsxy, U, V, sxy, i, j, st, 6);
+        if (P.g.py) dudy = (Uc(wrapi(j + 1, Ny)) - Uc(wrapi(j - 1, Ny))) / (2.0 * P.g.hy);
+        else if (j == 0) {
+            const SideD& s = P.bu.s[BOTTOM];
+            dudy = s.type == EFSI_BC_DIRICHLET ? (Uc(0) - wall_u_at_xc(s, i)) / (0.5 * P.g.hy) : -wall_u_at_xc(s, i);
+        } else if (j == Ny - 1) {
+            const SideD& s = P.bu.s[TOP];
+            dudy = s.type == EFSI_BC_DIRICHLET ? (wall_u_at_xc(s, i) - Uc(Ny - 1)) / (0.5 * P.g.hy) : wall_u_at_xc(s, i);
+        } else dudy = (Uc(j + 1) - Uc(j - 1)) / (2.0 * P.g.hy);
+        if (P.g.px) dvdx = (Vc(wrapi(i + 1, Nx)) - Vc(wrapi(i - 1, Nx))) / (2.0 * P.g.hx);
+        else if (i == 0) {
+            const SideD& s = P.bv.s[LEFT];
+            dvdx = s.type == EFSI_BC_DIRICHLET ? (Vc(0) - wall_u_at_xc(s, j)) / (0.5 * P.g.hx) : -wall_u_at_xc(s, j);
+        } else if (i == Nx - 1) {
+            const SideD& s = P.bv.s[RIGHT];
+            dvdx = s.type == EFSI_BC_DIRICHLET ? (wall_u_at_xc(s, j) - Vc(Nx - 1)) / (0.5 * P.g.hx) : wall_u_at_xc(s, j);
+        } else dvdx = (Vc(i + 1) - Vc(i - 1)) / (2.0 * P.g.hx);
+    }
+    const double dudx = (U[uidx(i + 1, j, Nx)] - U[uidx(i, j, Nx)]) * ihx;
+    const double dvdy = (V[vidx(i, j + 1, Nx)] - V[vidx(i, j, Nx)]) * ihy;
+    const double divv = dudx + dvdy;
     double kxx = 0, kxy = 0, kyx = 0, kyy = 0;
     if (G) growth_K(P.md, G[k], kxx, kxy, kyx, kyy);
     double a11 = dudx - kxx, a12 = dudy - kxy, a21 = dvdx - kyx, a22 = dvdy - kyy;
