@@ -41,7 +41,7 @@ FALLBACK_HBM_GBS = 6650.0
 # capture summarised in the named profile; None where no capture exists.
 MEASURED_TRAFFIC = {
     ("visc_cg", "fp64"): (145.0e6, "profiles/k_visc_cg_cavity_disks20_N1024.md"),
-    ("visc_cg", "mixed"): (66.8e6, "profiles/k_visc_mx_cavity_disks20_N1024_mixed.md"),
+    ("visc_cg", "mixed"): (67.3e6, "profiles/k_visc_mx_cavity_disks20_N1024_mixed.md"),
 }
 
 
