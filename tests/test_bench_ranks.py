@@ -60,3 +60,12 @@ def test_clock_summary_reports_median_under_load_and_reasons():
     out = s.summary()
     assert out["sm_mhz"] == 1965.0 and out["sm_max_mhz"] == 1965.0
     assert out["reasons"] == ["sw_power_cap"] and out["samples"] == 4
+
+
+def test_cpu_baseline_replicas_aggregate_over_processes():
+    """The CPU baseline runs one single-thread oracle replica per process and sums
+    their throughput."""
+    import argparse
+    a = argparse.Namespace(N=128, projection_reltol=1e-10, velocity_reltol=1e-8, steps=1)
+    v, done, el, n = bench.cpu_replicas(a, budget_s=2.0, max_steps=2, nproc=2)
+    assert n == 2 and done == 4 and v > 0.0 and el > 0.0
