@@ -1487,42 +1487,77 @@ __global__ void k_pcg_init(MGLevel L, int px, int py, double reltol, int maxiter
     }
 }
 
-// p = z + beta p_old, Kp, p.Kp -> alpha.  Persistent over 32x8 tiles; cells away from
-// the edges take the branch-free form of lev_diag/lev_off (same terms, same order).
+// Shared-memory view of p over one 32x8 tile with a one-cell halo: every slot holds
+// p at its wrapped global cell (zero outside walls), so the wrapped requests of
+// lev_off map back into the tile.
+struct TileP {
+    const double* sp;
+    int i0, j0, nx, ny;
+    __device__ __forceinline__ double operator()(int c, int r) const {
+        int lc = c - i0 + 1, lr = r - j0 + 1;
+        if (lc < 0) lc += nx; else if (lc >= VSX) lc -= nx;
+        if (lr < 0) lr += ny; else if (lr >= VSY) lr -= ny;
+        return sp[lr * VSX + lc];
+    }
+};
+
+// p = z + beta p_old, Kp, p.Kp -> alpha.  Persistent over 32x8 tiles; p is formed
+// once per cell of the tile and its halo in shared memory.  Cells away from the edges
+// take the branch-free form of lev_diag/lev_off (same terms, same order).
 __global__ void __launch_bounds__(BX * BY, 6) k_pcg_matvec(MGLevel L, int px, int py, const double* __restrict__ z,
                                                            const double* __restrict__ p_old, double* p, double* Ap,
                                                            CGScal* cg, RedSlot rs) {
+    static_assert(BX == VTX && BY == VTY, "the matvec tile is the viscous tile");
+    __shared__ double sp[VSX * VSY];
     __shared__ double sh[32];
     if (cg->done) return;
     const int first = cg->iter == 0;
     const int nx = L.nx, ny = L.ny;
     const double beta = first ? 0.0 : cg->beta;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + ty * BX;
     auto pn = [&](size_t k) { return first ? z[k] : z[k] + beta * p_old[k]; };
+    auto stage = [&](int gi, int gj) -> double {
+        const bool inx = gi >= 0 && gi < nx, iny = gj >= 0 && gj < ny;
+        if (!((inx || px) && (iny || py))) return 0.0;
+        return pn(cidx(inx ? gi : wrapm(gi, nx), iny ? gj : wrapm(gj, ny), nx));
+    };
     const int ntx = (nx + BX - 1) / BX, nt = ntx * ((ny + BY - 1) / BY);
     double acc[1] = {0.0};
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        const int i = (t % ntx) * BX + threadIdx.x, j = (t / ntx) * BY + threadIdx.y;
-        if (i >= nx || j >= ny) continue;
-        const size_t k = cidx(i, j, nx);
-        const double pc = pn(k);
-        double q;
-        if (i > 0 && i < nx - 1 && j > 0 && j < ny - 1) {
-            double d = 0.0;
-            d += L.ax; d += L.ax; d += L.ay; d += L.ay;
-            double off = 0.0;
-            off += L.ax * pn(k - 1);
-            off += L.ax * pn(k + 1);
-            off += L.ay * pn(k - nx);
-            off += L.ay * pn(k + nx);
-            q = d * pc - off;
-        } else {
-            double d;
-            lev_diag(L, px, py, i, j, d);
-            q = d * pc - lev_off(L, px, py, i, j, [&](int a, int c) { return pn(cidx(a, c, nx)); });
+        const int i0 = (t % ntx) * BX, j0 = (t / ntx) * BY;
+        const int i = i0 + tx, j = j0 + ty;
+        const bool own = i < nx && j < ny;
+        const int s = (ty + 1) * VSX + tx + 1;
+        const double pc = own ? pn(cidx(i, j, nx)) : stage(i, j);
+        sp[s] = pc;
+        if (tid < 2 * VSX + 2 * VTY) {
+            int lx, ly;
+            visc_halo_slot(tid, lx, ly);
+            sp[ly * VSX + lx] = stage(i0 + lx - 1, j0 + ly - 1);
         }
-        p[k] = pc;
-        Ap[k] = q;
-        acc[0] += pc * q;
+        __syncthreads();
+        if (own) {
+            const size_t k = cidx(i, j, nx);
+            double q;
+            if (i > 0 && i < nx - 1 && j > 0 && j < ny - 1) {
+                double d = 0.0;
+                d += L.ax; d += L.ax; d += L.ay; d += L.ay;
+                double off = 0.0;
+                off += L.ax * sp[s - 1];
+                off += L.ax * sp[s + 1];
+                off += L.ay * sp[s - VSX];
+                off += L.ay * sp[s + VSX];
+                q = d * pc - off;
+            } else {
+                double d;
+                lev_diag(L, px, py, i, j, d);
+                q = d * pc - lev_off(L, px, py, i, j, TileP{sp, i0, j0, nx, ny});
+            }
+            p[k] = pc;
+            Ap[k] = q;
+            acc[0] += pc * q;
+        }
+        __syncthreads();
     }
     double tot[1];
     if (grid_reduce<1>(acc, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0) {
