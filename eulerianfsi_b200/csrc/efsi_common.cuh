@@ -120,8 +120,9 @@ __device__ __forceinline__ double clamp01(double x) { return fmin(fmax(x, 0.0), 
 
 // ---- deterministic reductions ----------------------------------------------------------------
 // Block-level sum of NV values (blockDim.x*blockDim.y threads, multiple of 32).
-template <int NV>
-__device__ __forceinline__ void block_sum(double (&v)[NV], double* sh /* >= 32*NV */) {
+template <int NV, int M>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double (&sh)[M]) {
+    static_assert(M >= 32 * NV, "block reduction scratch needs 32 doubles per reduced value");
     const int tid = threadIdx.x + threadIdx.y * blockDim.x;
     const int nthr = blockDim.x * blockDim.y;
 #pragma unroll
@@ -143,8 +144,9 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* sh /* >= 32*N
     __syncthreads();
 }
 
-template <int NV>
-__device__ __forceinline__ void block_max(double (&v)[NV], double* sh) {
+template <int NV, int M>
+__device__ __forceinline__ void block_max(double (&v)[NV], double (&sh)[M]) {
+    static_assert(M >= 32 * NV, "block reduction scratch needs 32 doubles per reduced value");
     const int tid = threadIdx.x + threadIdx.y * blockDim.x;
     const int nthr = blockDim.x * blockDim.y;
 #pragma unroll
@@ -176,8 +178,8 @@ struct RedSlot {
     int maxBlocks;
 };
 
-template <int NV, bool MAXOP = false>
-__device__ bool grid_reduce(double (&v)[NV], const RedSlot& rs, double (&tot)[NV], double* sh) {
+template <int NV, bool MAXOP = false, int M>
+__device__ bool grid_reduce(double (&v)[NV], const RedSlot& rs, double (&tot)[NV], double (&sh)[M]) {
     const int tid = threadIdx.x + threadIdx.y * blockDim.x;
     const int nthr = blockDim.x * blockDim.y;
     const int nb = gridDim.x * gridDim.y;
