@@ -479,6 +479,7 @@ void build_projection(efsi_handle* h, const efsi_config& cfg) {
     pj.x = h->dalloc<double>(N); pj.r[0] = h->dalloc<double>(N); pj.r[1] = h->dalloc<double>(N); pj.z = pj.lev[0].xo;
     pj.p[0] = h->dalloc<double>(N); pj.p[1] = h->dalloc<double>(N);
     pj.Ap = h->dalloc<double>(N); pj.b = h->dalloc<double>(N); pj.rhs = h->dalloc<double>(N);
+    pj.w = h->dalloc<double>(N); pj.s[0] = h->dalloc<double>(N); pj.s[1] = h->dalloc<double>(N);
     pj.Up = h->dalloc<double>(h->nu); pj.Vp = h->dalloc<double>(h->nv);
 }
 
@@ -642,7 +643,8 @@ void projection(efsi_handle* h, bool compact, const double* u_in, const double* 
     const double vb = proj_update_vcycle_bytes(h->pj);
     const int vk = proj_update_vcycle_kernels(h->pj);
     solve(
-        h, KIND_PROJ, stage_slot, &d->cg_proj, P.nu.projection_maxiter, 2 * (1 + vk), 2,
+        h, KIND_PROJ, stage_slot, &d->cg_proj, P.nu.projection_maxiter,
+        2 * (proj_matvec_kernels(h->pj) + vk), 2,
         [&](cudaStream_t s, int* io, cudaGraphConditionalHandle ch) {
             proj_cg_init(P, h->pj, P.nu.projection_reltol, P.nu.projection_maxiter, h->q, &d->cg_proj, &d->ps,
                          h->slot[1], h->slot[2], &d->st, io, ch, s);

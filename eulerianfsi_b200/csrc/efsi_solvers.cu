@@ -976,13 +976,19 @@ __device__ __forceinline__ bool inner_tile(const MGLevel& L, int i0, int j0, int
     return i0 - H >= 1 && i0 + T + H <= L.nx - 1 && j0 - H >= 1 && j0 + T + H <= L.ny - 1;
 }
 
-// CG update fused into the finest pre-smoothing: r_new = r_old - a Kp, x += a p.
+// Chronopoulos-Gear CG update fused into the finest pre-smoothing (z = M r and w = K z
+// of the previous V-cycle):  p = z + b p_old, s = w + b s_old, x += a p,
+// r_new = r_old - a s  (first iteration: p = z, s = w).
 struct CGFuse {
     const double* r_old;
-    const double* Ap;
-    const double* p;
+    const double* w;
+    const double* s_old;
+    const double* z;
+    const double* p_old;
     double* x;
     double* r_new;
+    double* s_new;
+    double* p_new;
 };
 
 // Down leg of one level: pre-smoothing from x = 0 (red x = b/D, then one black GS
@@ -1006,6 +1012,8 @@ __global__ void __launch_bounds__(256, 4) k_mg_down(MGLevel L, MGLevel C, int px
     const int tid = threadIdx.x;
     const int nx = L.nx;
     const double a = FUSE ? cg->alpha : 0.0;
+    const bool first = FUSE && cg->iter == 0;
+    const double bt = FUSE && !first ? cg->beta : 0.0;
     const double d0 = inner_diag(L);
     double acc[1] = {0.0};
     const int ntx = (nx + T - 1) / T, nt = ntx * ((L.ny + T - 1) / T);
@@ -1033,7 +1041,12 @@ __global__ void __launch_bounds__(256, 4) k_mg_down(MGLevel L, MGLevel C, int px
                 k = cidx(sp.wi, sp.wj, nx);
                 lev_diag(L, px, py, sp.wi, sp.wj, vd[q]);
             }
-            vb[q] = FUSE ? __ldg(f.r_old + k) - a * __ldg(f.Ap + k) : (double)__ldg(b + k);
+            if (FUSE) {
+                const double sv = first ? __ldg(f.w + k) : __ldg(f.w + k) + bt * __ldg(f.s_old + k);
+                vb[q] = __ldg(f.r_old + k) - a * sv;
+            } else {
+                vb[q] = (double)__ldg(b + k);
+            }
         }
 #pragma unroll
         for (int q = 0; q < NS; ++q) {
@@ -1045,9 +1058,9 @@ __global__ void __launch_bounds__(256, 4) k_mg_down(MGLevel L, MGLevel C, int px
             sx[s] = (vd[q] != 0.0 && ((lx + ly) & 1) == 0) ? vb[q] / vd[q] : 0.0;
         }
         __syncthreads();
-        if (FUSE) {  // owned cells: r_new, x += a p, |r_new|^2
+        if (FUSE) {  // owned cells: p, s, x += a p, r_new, |r_new|^2
             constexpr int NO = T * T / 256;
-            double pv[NO], xv[NO];
+            double pv[NO], sv[NO], xv[NO];
             size_t kk[NO];
             bool in[NO];
 #pragma unroll
@@ -1055,14 +1068,21 @@ __global__ void __launch_bounds__(256, 4) k_mg_down(MGLevel L, MGLevel C, int px
                 const int s = tid + q * 256, lx = s % T, ly = s / T;
                 in[q] = i0 + lx < nx && j0 + ly < L.ny;
                 kk[q] = cidx(i0 + lx, j0 + ly, nx);
-                pv[q] = in[q] ? f.p[kk[q]] : 0.0;
-                xv[q] = in[q] ? f.x[kk[q]] : 0.0;
+                pv[q] = 0.0;
+                sv[q] = 0.0;
+                xv[q] = 0.0;
+                if (!in[q]) continue;
+                pv[q] = first ? f.z[kk[q]] : f.z[kk[q]] + bt * f.p_old[kk[q]];
+                sv[q] = first ? f.w[kk[q]] : f.w[kk[q]] + bt * f.s_old[kk[q]];
+                xv[q] = f.x[kk[q]];
             }
 #pragma unroll
             for (int q = 0; q < NO; ++q) {
                 if (!in[q]) continue;
                 const int s = tid + q * 256, lx = s % T, ly = s / T;
                 const double v = sb[(ly + H) * W + lx + H];
+                f.p_new[kk[q]] = pv[q];
+                f.s_new[kk[q]] = sv[q];
                 f.r_new[kk[q]] = v;
                 f.x[kk[q]] = xv[q] + a * pv[q];
                 acc[0] += v * v;
@@ -1134,21 +1154,24 @@ __global__ void __launch_bounds__(256, 4) k_mg_down(MGLevel L, MGLevel C, int px
 }
 
 // Up leg of one level: x + P e (bilinear prolongation), then the post-smoothing
-// black-then-red Gauss-Seidel sweep; on the finest level also r.z for CG.
+// black-then-red Gauss-Seidel sweep.  DOT (finest level, the CG preconditioner):
+// z is completed over the tile and a one-cell ring, w = K z is formed on the tile,
+// and the Chronopoulos-Gear scalars follow from g = r.z and d = z.w:
+//   first V-cycle of a solve: a = g / d;  otherwise b = g / g_old, a = g / (d - b g / a_old).
 template <int T, bool DOT, class S, class IN, class OUT>
 __global__ void __launch_bounds__(256, 4) k_mg_up(MGLevel L, MGLevel C, int px, int py, const S* __restrict__ x,
                                                   const S* __restrict__ e, const IN* __restrict__ b, OUT* xo,
-                                                  CGScal* cg, RedSlot rs) {
-    constexpr int H = 2, W = T + 2 * H;
+                                                  double* wo, CGScal* cg, RedSlot rs) {
+    constexpr int H = DOT ? 3 : 2, W = T + 2 * H;
     __shared__ double sx[W * W];
     __shared__ double sb[W * W];
     __shared__ double sd[W * W];
-    __shared__ double sh[32];
+    __shared__ double sh[2 * 32];  // block sums of r.z and z.w
     if (cg && cg->done) return;
     const int tid = threadIdx.x;
     const int nx = L.nx;
     const double d0 = inner_diag(L);
-    double acc[1] = {0.0};
+    double acc[2] = {0.0, 0.0};
     const int ntx = (nx + T - 1) / T, nt = ntx * ((L.ny + T - 1) / T);
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const int i0 = (t % ntx) * T, j0 = (t / ntx) * T;
@@ -1185,10 +1208,11 @@ __global__ void __launch_bounds__(256, 4) k_mg_up(MGLevel L, MGLevel C, int px, 
             sd[s] = dv[q];
         }
         __syncthreads();
-        // black cells within halo 1
-        constexpr int B = T + 2;
+        // black cells within halo H - 1 (a slot's colour is the parity of lx + ly: tile
+        // origins are even, so it does not depend on H)
+        constexpr int B = T + 2 * (H - 1);
         for (int s = tid; s < B * B / 2; s += 256) {
-            const int ry = s / (B / 2), rx = 2 * (s % (B / 2)) + ((ry + 1) & 1);
+            const int ry = s / (B / 2), rx = 2 * (s % (B / 2)) + ((ry + 1) & 1);  // lx + ly odd
             const int lx = rx + 1, ly = ry + 1, k = ly * W + lx;
             const double d = sd[k];
             if (d == 0.0) continue;
@@ -1197,6 +1221,37 @@ __global__ void __launch_bounds__(256, 4) k_mg_up(MGLevel L, MGLevel C, int px, 
             sx[k] = (sb[k] + off) / d;
         }
         __syncthreads();
+        if (DOT) {
+            // red cells of the tile and its one-cell ring (their black neighbours are final)
+            constexpr int R = T + 2;
+            for (int s = tid; s < R * R / 2; s += 256) {
+                // lx + ly even; lx = rx + H - 1 and ly = ry + H - 1 with H - 1 = 2 even
+                const int ry = s / (R / 2), rx = 2 * (s % (R / 2)) + (ry & 1);
+                const int lx = rx + H - 1, ly = ry + H - 1, k = ly * W + lx;
+                const double d = sd[k];
+                if (d == 0.0) continue;
+                const double off = inner ? inner_off(L, sx, k, W)
+                                         : slot_off(L, px, py, i0 + lx - H, j0 + ly - H, sx, k, W);
+                sx[k] = (sb[k] + off) / d;
+            }
+            __syncthreads();
+            // z on the tile, w = K z, r.z and z.w
+            for (int s = tid; s < T * T; s += 256) {
+                const int lx = s % T, ly = s / T;
+                const int gi = i0 + lx, gj = j0 + ly;
+                if (gi >= nx || gj >= L.ny) continue;
+                const int k = (ly + H) * W + lx + H;
+                const double zc = sx[k];
+                const double off = inner ? inner_off(L, sx, k, W) : slot_off(L, px, py, gi, gj, sx, k, W);
+                const double wc = sd[k] * zc - off;
+                xo[cidx(gi, gj, nx)] = (OUT)zc;
+                wo[cidx(gi, gj, nx)] = wc;
+                acc[0] += sb[k] * zc;
+                acc[1] += zc * wc;
+            }
+            __syncthreads();
+            continue;
+        }
         // red cells of the tile (their black neighbours are final); write the tile
         for (int s = tid; s < T * T; s += 256) {
             const int lx = s % T, ly = s / T;
@@ -1210,15 +1265,24 @@ __global__ void __launch_bounds__(256, 4) k_mg_up(MGLevel L, MGLevel C, int px, 
                 val = (bc + off) / sd[k];
             }
             xo[cidx(gi, gj, nx)] = (OUT)val;
-            acc[0] += bc * val;
         }
         __syncthreads();
     }
     if (!DOT) return;
-    double tot[1];
-    if (grid_reduce<1>(acc, rs, tot, sh) && tid == 0) {
-        cg->beta = cg->rz != 0.0 ? tot[0] / cg->rz : 0.0;
-        cg->rz = tot[0];
+    double tot[2];
+    if (grid_reduce<2>(acc, rs, tot, sh) && tid == 0) {
+        const double g = tot[0], d = tot[1];
+        if (cg->iter == 0) {
+            cg->beta = 0.0;
+            cg->alpha = d != 0.0 ? g / d : 0.0;
+        } else {
+            const double bn = cg->rz != 0.0 ? g / cg->rz : 0.0;
+            const double den = d - (cg->alpha != 0.0 ? bn * g / cg->alpha : 0.0);
+            cg->beta = bn;
+            cg->alpha = den != 0.0 ? g / den : 0.0;
+        }
+        cg->rz = g;
+        cg->pAp = d;
     }
 }
 
@@ -1314,10 +1378,11 @@ static void mg_up(const Projection& pj, const MGLevel& L, const MGLevel& C, int 
                   CGScal* cg, const RedSlot& rs2, int px, int py, cudaStream_t s) {
     using A = LevelArrays<S>;
     if (l == 0)
-        k_mg_up<T, true, S, double, double><<<grid, 256, 0, s>>>(L, C, px, py, A::x(L), A::xo(C), r_fine, pj.z, cg,
-                                                                rs2);
+        k_mg_up<T, true, S, double, double><<<grid, 256, 0, s>>>(L, C, px, py, A::x(L), A::xo(C), r_fine, pj.z,
+                                                                pj.w, cg, rs2);
     else
-        k_mg_up<T, false, S, S, S><<<grid, 256, 0, s>>>(L, C, px, py, A::x(L), A::xo(C), A::b(L), A::xo(L), cg, rs2);
+        k_mg_up<T, false, S, S, S><<<grid, 256, 0, s>>>(L, C, px, py, A::x(L), A::xo(C), A::b(L), A::xo(L),
+                                                        nullptr, cg, rs2);
 }
 
 template <class S>
@@ -1360,14 +1425,15 @@ static void vcycle(const Projection& pj, const double* r_fine, const CGFuse* fus
 }
 
 int proj_update_vcycle_kernels(const Projection& pj) { return pj.nlev == 1 ? 3 : 2 * (pj.nlev - 1) + 1; }
+int proj_matvec_kernels(const Projection& pj) { return pj.nlev == 1 ? 1 : 0; }
 int proj_init_kernels(const Projection& pj) { return 1 + (pj.nlev == 1 ? 2 : 2 * (pj.nlev - 1) + 1); }
 double proj_update_vcycle_bytes(const Projection& pj) {
     const double n0 = (double)pj.lev[0].nx * pj.lev[0].ny;
     if (pj.nlev == 1) return 8.0 * (6.0 * n0 + (double)pj.nc * pj.nc + 4.0 * pj.nc);
     const double e = pj.mixed ? 4.0 : 8.0;  // bytes of a multigrid level element
-    // finest: r_old, Kp, p, x read and x, r_new written (FP64); L.x and C.b written;
-    // up: L.x, e read, r_new read (FP64), z written (FP64)
-    double b = 8.0 * 8.0 * n0 + e * (2.25 * n0 + 0.25 * n0 + 1.0 * n0);
+    // finest down: r_old, w, s_old, z, p_old, x read and p, s, x, r_new written (FP64);
+    // L.x and C.b written; up: L.x, e read, r_new read, z and w written (FP64)
+    double b = 8.0 * 13.0 * n0 + e * (2.25 * n0 + 0.25 * n0 + 1.0 * n0);
     for (int l = 1; l + 1 < pj.nlev; ++l) b += e * 5.5 * (double)pj.lev[l].nx * pj.lev[l].ny;
     b += e * ((double)pj.nc * pj.nc + 2.0 * pj.nc);
     return b;
@@ -1604,6 +1670,7 @@ void proj_cg_init(const Params& P, const Projection& pj, double reltol, int maxi
 // One CG iteration is proj_matvec then proj_update_vcycle with the same parity:
 // p[parity] is written, r[parity] is read and r[parity^1] written (multigrid case).
 void proj_matvec(const Params& P, const Projection& pj, int parity, CGScal* cg, const RedSlot& rs, cudaStream_t s) {
+    if (pj.nlev > 1) return;  // the multigrid V-cycle forms w = K z itself (Chronopoulos-Gear)
     const MGLevel& L = pj.lev[0];
     const int cur = parity & 1, old = cur ^ 1;
     const int nt = ((L.nx + BX - 1) / BX) * ((L.ny + BY - 1) / BY);
@@ -1620,8 +1687,9 @@ void proj_update_vcycle(const Params& P, const Projection& pj, int parity, CGSca
         vcycle(pj, pj.r[0], nullptr, cg, rs, rs2, nullptr, 0, P.g.px, P.g.py, s);
         return;
     }
-    const CGFuse f{pj.r[cur], pj.Ap, pj.p[cur], pj.x, pj.r[cur ^ 1]};
-    vcycle(pj, pj.r[cur ^ 1], &f, cg, rs, rs2, iters_out, cond, P.g.px, P.g.py, s);
+    const int old = cur ^ 1;
+    const CGFuse f{pj.r[cur], pj.w, pj.s[old], pj.z, pj.p[old], pj.x, pj.r[old], pj.s[cur], pj.p[cur]};
+    vcycle(pj, pj.r[old], &f, cg, rs, rs2, iters_out, cond, P.g.px, P.g.py, s);
 }
 
 // ---- correction and diagnostics (Projection.jl:253-306) ---------------------------------------

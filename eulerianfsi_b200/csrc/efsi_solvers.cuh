@@ -76,8 +76,9 @@ struct Projection {
     bool nullspace;
     bool mixed;           // precision form: multigrid levels stored and applied in FP32
     int nsm;              // multiprocessors (persistent launch grids)
-    // fine-level CG vectors (r ping-pongs between iterations when multigrid levels exist)
-    double *x, *r[2], *z, *p[2], *Ap, *b, *rhs;
+    // fine-level CG vectors (r, p and s ping-pong between iterations when multigrid
+    // levels exist; w = K z, s = w + beta s_old in the Chronopoulos-Gear recurrence)
+    double *x, *r[2], *z, *p[2], *Ap, *b, *rhs, *w, *s[2];
     double *Up, *Vp;      // predictor velocity (full MAC arrays)
 };
 // Per-projection scalars: [0] defect, [1] scale, [2] sum b, [3] |rhs|^2, [4] wl2(div)^2,
@@ -91,8 +92,12 @@ void proj_rhs(const Params& P, const Projection& pj, bool compact_in, const doub
 void proj_cg_init(const Params& P, const Projection& pj, double reltol, int maxiter, const double* q0, CGScal* cg,
                   const ProjScal* ps, const RedSlot& rs, const RedSlot& rs2, const DevStatus* st, int* iters_out,
                   cudaGraphConditionalHandle cond, cudaStream_t s);
+// Standard PCG p and Kp on a single-level (dense) hierarchy; nothing with multigrid levels.
 void proj_matvec(const Params& P, const Projection& pj, int parity, CGScal* cg, const RedSlot& rs, cudaStream_t s);
-// CG update (x += a p, r -= a Kp, convergence) fused with the multigrid V-cycle z = M r.
+int proj_matvec_kernels(const Projection& pj);
+// CG update fused with the multigrid V-cycle z = M r: Chronopoulos-Gear with levels (p, s,
+// x, r updated in the finest down leg; w = K z and both inner products in the finest up
+// leg), standard PCG (x += a p, r -= a Kp) on a single dense level.
 void proj_update_vcycle(const Params& P, const Projection& pj, int parity, CGScal* cg, const RedSlot& rs,
                         const RedSlot& rs2, int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s);
 void proj_finish(const Params& P, const Projection& pj, const double* G, double* q_out, double* U_out,
