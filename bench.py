@@ -40,7 +40,7 @@ FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from the ncu
 # capture summarised in the named profile; None where no capture exists.
 MEASURED_TRAFFIC = {
-    ("visc_cg", "fp64"): (145.0e6, "profiles/k_visc_cg_cavity_disks20_N1024.md"),
+    ("visc_cg", "fp64"): (144.3e6, "profiles/k_visc_cg_cavity_disks20_N1024.md"),
     ("visc_cg", "mixed"): (67.3e6, "profiles/k_visc_mx_cavity_disks20_N1024_mixed.md"),
 }
 
