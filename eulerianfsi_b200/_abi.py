@@ -10,7 +10,7 @@ import ctypes as C
 import os
 from ctypes import POINTER, Structure, c_char_p, c_double, c_int32, c_int64, c_uint8, c_void_p
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # status codes
 OK, ARG, DIM, SOLVE, DOMAIN, CUDA, UNSUPPORTED = range(7)
@@ -31,6 +31,9 @@ NORMALS_STANDARD, NORMALS_YOUNGS, NORMALS_SMOOTHED9 = range(3)
 FORCE_NONE, FORCE_CONSTANT, FORCE_KOLMOGOROV = range(3)
 EXT_NONE, EXT_IDENTITY_OUTSIDE, EXT_GEOMETRIC = range(3)
 PRECISION_FP64, PRECISION_MIXED = range(2)
+LINEAR_DIRECT, LINEAR_GMRES = range(2)
+LINEAR_HARD_CAP = 10000
+STEP_GRAPH, STEP_HOST = range(2)
 
 _dp = POINTER(c_double)
 
@@ -79,7 +82,8 @@ class Numerics(Structure):
         ("stage1_constraint_atol", c_double), ("stage1_constraint_rtol", c_double),
         ("check_stage1_constraint", c_int32),
         ("linear_reltol", c_double), ("linear_maxiter", c_int32),
-        ("precision", c_int32), ("reserved", c_int32 * 7),
+        ("precision", c_int32), ("velocity_method", c_int32), ("resource_method", c_int32),
+        ("direct_fallback", c_int32), ("fallback_reltol", c_double), ("reserved", c_int32 * 4),
     ]
 
 
@@ -111,7 +115,7 @@ class Stats(Structure):
     _fields_ = [("projection_iterations", c_int32 * 4), ("velocity_iterations", c_int32 * 4),
                 ("resource_iterations", c_int32 * 4), ("kernel_launches", c_int64),
                 ("device_ms", c_double), ("site_launches", c_int64), ("site_ms", c_double),
-                ("site_bytes", c_double)]
+                ("site_bytes", c_double), ("step_bytes", c_double)]
 
 
 DIAG_MAX_MODES = 8
@@ -171,6 +175,7 @@ SIGNATURES = {
 }
 CUDA_ONLY = {
     "set_timed_site": (c_int32, [_H, c_int32]),
+    "set_step_mode": (c_int32, [_H, c_int32]),
     "integrate_step_host": (c_int32, [_H] + [_dp] * 8 + [c_double, c_double, POINTER(StepReportC)]),
     "step_n": (c_int32, [_H, c_double, _dp, c_int32, POINTER(StepReportC)]),
     # no handle: device pointers in, device result out (allocates nothing)

@@ -8,7 +8,7 @@
 // residual test passes, so a step is one graph launch and a batch of steps needs
 // one host synchronisation.  (t, dt) come from a device array indexed by a step
 // counter, so the same graph serves every step.  When a launch site is being timed
-// (or EFSI_STEP_GRAPH=0) the step is enqueued from the host instead, with the solves
+// (or efsi_set_step_mode selects EFSI_STEP_HOST) the step is enqueued from the host instead, with the solves
 // in batches sized from the previous solve's iteration count.  Device-side errors
 // (the Julia exceptions of the reference) are raised into a status word and
 // reported after the step; a failing step leaves the state untouched.
@@ -126,6 +126,7 @@ struct efsi_handle {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> site_ev;
     size_t site_used = 0;
     double site_bytes_pending = 0.0;
+    double step_bytes_pending = 0.0;  // algorithmic bytes of every site launch (host-driven)
 
     template <class T>
     T* dalloc(size_t n) {
@@ -171,6 +172,7 @@ void reset_call_stats(efsi_handle* h) {
 // Bracket a launch site with CUDA events when it is the timed one.
 template <class F>
 void site(efsi_handle* h, int which, double bytes, F&& f) {
+    if (!h->capturing) h->step_bytes_pending += bytes;
     if (h->capturing || h->timed_site != which) { f(); return; }
     if (h->site_used == h->site_ev.size()) {
         cudaEvent_t a, b;
@@ -194,8 +196,10 @@ void collect_site_events(efsi_handle* h) {
         h->stats.site_launches += 1;
     }
     h->stats.site_bytes += h->site_bytes_pending;
+    h->stats.step_bytes += h->step_bytes_pending;
     h->site_used = 0;
     h->site_bytes_pending = 0.0;
+    h->step_bytes_pending = 0.0;
 }
 
 void call_begin(efsi_handle* h) { check_cuda(cudaEventRecord(h->call_ev[0], h->stream), "event"); }
@@ -527,9 +531,9 @@ Err decode(const DevStatus& s) {
         case DE_BAD_VISCOSITY: return {EFSI_ARG, "evaluated viscosity must be strictly positive everywhere."};
         case DE_BAD_DIFFUSIVITY: return {EFSI_ARG, "evaluated diffusivity must be strictly positive everywhere."};
         case DE_NONFINITE_SINK: return {EFSI_ARG, "Evaluated resource sink contains non-finite values."};
-        case DE_LINEAR_NOCONV:
-            snprintf(buf, sizeof buf, "%s linear solve did not converge (residual %.3g).",
-                     s.where == 0 ? "velocity" : (s.where == 1 ? "resource" : "projection"), s.value);
+        case DE_LINEAR_NOCONV:  // _solve_linear_system! (TimeIntegrationIMEX.jl:637), stage numbered from 1
+            snprintf(buf, sizeof buf, "%s stage %d GMRES residual is too large: %.17g",
+                     s.where == 0 ? "velocity" : "resource", s.i + 1, s.value);
             return {EFSI_SOLVE, buf};
         default:
             snprintf(buf, sizeof buf, "device error %d", s.code);
@@ -696,6 +700,9 @@ void tendencies(efsi_handle* h, int s, const StageFields& f) {
 
 const double c_AI_diag[4] = {0.0, 4.0 / 15, 1.0 / 15, 1.0 / 6};
 
+// Iterations a host-driven solve may enqueue: its limit plus the DIRECT continuation.
+int solve_limit(const SolveOpts& o) { return o.maxiter + (o.fallback ? EFSI_LINEAR_HARD_CAP : 0); }
+
 // The whole IMEX step (TimeIntegrationIMEX.jl:1159-1255) for the (t, dt) at the
 // batch counter; identical for every step so that it can be captured once.
 void enqueue_step(efsi_handle* h) {
@@ -726,18 +733,20 @@ void enqueue_step(efsi_handle* h) {
                 cstage = h->cs;
                 if (h->diff) {
                     DtCoef alpha{dtp, c_AI_diag[st]};
-                    const int maxit = std::max(1, P.nu.linear_maxiter);
+                    const SolveOpts o = solve_opts(P.nu, P.nu.resource_method);
                     solve(
-                        h, KIND_DIFF, st, &d->cg_diff, maxit, 6, 2,
+                        h, KIND_DIFF, st, &d->cg_diff, solve_limit(o), 6, 2,
                         [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
-                            diff_init(P, alpha, P.nu.linear_reltol, maxit, h->c, h->rhs_c, h->phis, h->ds,
-                                      &d->cg_diff, h->slot[0], io, ch, ss);
+                            diff_init(P, alpha, o, h->c, h->rhs_c, h->phis, h->ds, &d->cg_diff, h->slot[0], io, ch,
+                                      ss);
                             h->launches += 1;
                         },
                         [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
                             for (int k = 0; k < 2; ++k)
                                 diff_iter(P, alpha, h->phis, h->ds, &d->cg_diff, h->slot[1], h->slot[2], io, ch, ss);
                         });
+                    solve_status(&d->cg_diff, &d->st, 1, st, s);
+                    h->launches += 1;
                 }
             }
             f = StageFields{h->Us, h->Vs, h->phis, cstage, h->sxs, h->sys, h->sxys, Gp};
@@ -757,14 +766,15 @@ void enqueue_step(efsi_handle* h) {
             h->launches += 1;
             if (h->visc) {
                 DtCoef alpha{dtp, c_AI_diag[st]};
-                const int maxit = std::max(1, P.nu.linear_maxiter);
+                const SolveOpts o = solve_opts(P.nu, P.nu.velocity_method);
+                const int maxit = solve_limit(o);
                 if (h->mixed) {
                     solve(
                         h, KIND_VISC, st, &d->cg_visc, maxit, 2, 2,
                         [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
                             site(h, EFSI_SITE_VISC_INIT, 8.0 * N * 10.0, [&] {
-                                visc_mx_init(P, alpha, P.nu.linear_reltol, maxit, h->U, h->V, h->rhs_u, h->rhs_v,
-                                             h->phis, h->vs, h->vm, &d->cg_visc, h->slot[0], io, ch, ss);
+                                visc_mx_init(P, alpha, o, h->U, h->V, h->rhs_u, h->rhs_v, h->phis, h->vs, h->vm,
+                                             &d->cg_visc, h->slot[0], io, ch, ss);
                             });
                             h->launches += 2;
                         },
@@ -780,8 +790,8 @@ void enqueue_step(efsi_handle* h) {
                     h, KIND_VISC, st, &d->cg_visc, maxit, 2, 2,
                     [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
                         site(h, EFSI_SITE_VISC_INIT, 8.0 * N * 18.0, [&] {
-                            visc_init(P, alpha, P.nu.linear_reltol, maxit, h->U, h->V, h->rhs_u, h->rhs_v, h->phis,
-                                      h->vs, &d->cg_visc, h->slot[0], h->slot[1], io, ch, ss);
+                            visc_init(P, alpha, o, h->U, h->V, h->rhs_u, h->rhs_v, h->phis, h->vs, &d->cg_visc,
+                                      h->slot[0], h->slot[1], io, ch, ss);
                         });
                         h->launches += 3;
                     },
@@ -791,6 +801,8 @@ void enqueue_step(efsi_handle* h) {
                                 visc_iter(P, alpha, h->phis, h->vs, k, &d->cg_visc, h->slot[2], io, ch, ss);
                             });
                     });
+                solve_status(&d->cg_visc, &d->st, 0, st, s);
+                h->launches += 1;
             } else {
                 visc_enforce_dirichlet(P, h->rhs_u, h->rhs_v, h->vs.x_u, h->vs.x_v, s);
                 h->launches += 1;
@@ -879,7 +891,7 @@ void run_steps(efsi_handle* h, double t0, const double* dts, int n, efsi_step_re
     } else {
         ensure_graph(h);
     }
-    const bool graph = h->step_exec && h->timed_site == EFSI_SITE_NONE;
+    const bool graph = h->use_graph && h->step_exec && h->timed_site == EFSI_SITE_NONE;
     long long launches = 0;
     int32_t its[3][4] = {};
     k_reset_call<<<1, 1, 0, h->stream>>>(h->dev);
@@ -1017,6 +1029,11 @@ int efsi_create(const efsi_config* cfg, efsi_handle** out) {
         if (!(P.nu.projection_reltol > 0)) throw Err{EFSI_ARG, "projection_reltol must be positive."};
         if (!(P.nu.projection_maxiter > 0)) throw Err{EFSI_ARG, "projection_maxiter must be positive."};
         if (!(P.nu.linear_reltol > 0)) throw Err{EFSI_ARG, "Linear-solver reltol must be positive."};
+        if (!(P.nu.linear_maxiter > 0)) throw Err{EFSI_ARG, "Linear-solver maxiter must be positive."};
+        if (!(P.nu.fallback_reltol > 0)) throw Err{EFSI_ARG, "fallback_reltol must be positive."};
+        for (int m : {P.nu.velocity_method, P.nu.resource_method})
+            if (m != EFSI_LINEAR_DIRECT && m != EFSI_LINEAR_GMRES)
+                throw Err{EFSI_ARG, "velocity_method must be :direct or :gmres."};
         h->visc = P.md.viscosity != EFSI_VISC_NONE;
         h->diff = P.md.diffusivity != EFSI_DIFF_NONE;
         h->growth = P.md.growth_source != EFSI_GROWTH_NONE;
@@ -1095,7 +1112,6 @@ int efsi_create(const efsi_config* cfg, efsi_handle** out) {
         check_cuda(cudaMallocHost(&h->times_pinned, 2 * (size_t)kMaxBatch * sizeof(double)), "pinned");
         check_cuda(cudaMallocHost(&h->hist_pinned, (size_t)kMaxBatch * sizeof(StepRec)), "pinned");
         check_cuda(cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking), "stream");
-        if (const char* e = std::getenv("EFSI_STEP_GRAPH")) h->use_graph = std::strcmp(e, "0") != 0;
         // default state: rest, sigma = I (the workspace's initial values)
         std::vector<double> ones(N, 1.0);
         check_cuda(cudaMemcpy(h->sxx, ones.data(), N * sizeof(double), cudaMemcpyHostToDevice), "init");
@@ -1434,6 +1450,13 @@ int efsi_state_diagnostics(efsi_handle* h, const efsi_diag_config* cfg, efsi_dia
     });
 }
 
+int efsi_set_step_mode(efsi_handle* h, int32_t mode) {
+    return guarded(h, [&] {
+        if (mode != EFSI_STEP_GRAPH && mode != EFSI_STEP_HOST) throw Err{EFSI_ARG, "unknown step mode"};
+        h->use_graph = mode == EFSI_STEP_GRAPH;
+    });
+}
+
 int efsi_set_timed_site(efsi_handle* h, int32_t which) {
     return guarded(h, [&] {
         if (which < EFSI_SITE_NONE || which >= EFSI_SITE_COUNT) throw Err{EFSI_ARG, "unknown launch site"};
@@ -1441,8 +1464,10 @@ int efsi_set_timed_site(efsi_handle* h, int32_t which) {
         h->stats.site_launches = 0;
         h->stats.site_ms = 0.0;
         h->stats.site_bytes = 0.0;
+        h->stats.step_bytes = 0.0;
         h->site_used = 0;
         h->site_bytes_pending = 0.0;
+        h->step_bytes_pending = 0.0;
     });
 }
 
@@ -1492,7 +1517,9 @@ void require_device_pointer(const void* p, int device, const char* name) {
 }
 
 // Same arithmetic as the stage-1 check of the step (k_stage1_check): per cell
-// |(U(i+1)-U(i))/hx + (V(j+1)-V(j))/hy - G| and |G|, max-reduced over the grid.
+// |(U(i+1)-U(i))/hx + (V(j+1)-V(j))/hy - G| and |G|, max-reduced over the grid.  The
+// max reduction (fmax) would drop a NaN, so a non-finite cell value enters as +Inf:
+// a velocity or target holding NaN or Inf can never report a finite residual.
 __global__ void k_div_residual_noalloc(int Nx, int Ny, double ihx, double ihy, const double* __restrict__ U,
                                        const double* __restrict__ V, const double* __restrict__ G, double* out,
                                        RedSlot rs) {
@@ -1502,8 +1529,9 @@ __global__ void k_div_residual_noalloc(int Nx, int Ny, double ihx, double ihy, c
     if (i < Nx && j < Ny) {
         double div = (U[uidx(i + 1, j, Nx)] - U[uidx(i, j, Nx)]) * ihx + (V[vidx(i, j + 1, Nx)] - V[vidx(i, j, Nx)]) * ihy;
         double g = G ? G[cidx(i, j, Nx)] : 0.0;
-        v[0] = fabs(div - g);
-        v[1] = fabs(g);
+        const double r = fabs(div - g), a = fabs(g);
+        v[0] = isfinite(r) ? r : INFINITY;
+        v[1] = isfinite(a) ? a : INFINITY;
     }
     double tot[2];
     if (grid_reduce<2, true>(v, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0) {

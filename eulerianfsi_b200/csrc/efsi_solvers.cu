@@ -91,6 +91,25 @@ __device__ __forceinline__ bool v_fixed(const Params& P, int j) {
     return !P.g.py && j == 0 && P.bv.s[BOTTOM].type == EFSI_BC_DIRICHLET;
 }
 
+// Start-of-solve scalars of a velocity / resource CG from the squared initial residual
+// rr0 and |b|^2; a non-finite start fails at once.
+__device__ __forceinline__ void cg_begin(CGScal* cg, const SolveOpts& o, double rr0, double bnorm2) {
+    cg->tol2 = o.reltol * o.reltol * rr0;
+    cg->iter = 0;
+    cg->maxiter = o.maxiter;
+    cg->alpha = 0.0;
+    cg->beta = 0.0;
+    cg->bnorm2 = bnorm2;
+    cg->fb_tol = o.fb_tol;
+    cg->fallback = o.fallback;
+    cg->in_fallback = 0;
+    cg->fail_rel = 0.0;
+    cg->conv = rr0 == 0.0 ? 1 : 0;
+    cg->fail = isfinite(rr0) && isfinite(bnorm2) ? 0 : 1;
+    if (cg->fail) cg->fail_rel = NAN;
+    cg->done = (cg->conv || cg->fail) ? 1 : 0;
+}
+
 // x0 = uv_n with the Dirichlet rows set to their data (the reference's GMRES start,
 // TimeIntegrationIMEX.jl:807, after _impose_row_dirichlet).
 __global__ void k_visc_x0(Params P, const double* __restrict__ Un, const double* __restrict__ Vn, double* xu,
@@ -103,15 +122,15 @@ __global__ void k_visc_x0(Params P, const double* __restrict__ Un, const double*
     xv[k] = v_fixed(P, j) ? bval(P.bv.s[BOTTOM], i) : Vn[vidx(i, j, Nx)];
 }
 
-__global__ void k_visc_init(Params P, DtCoef ac, double reltol, int maxiter, const double* __restrict__ xu,
+__global__ void k_visc_init(Params P, DtCoef ac, SolveOpts o, const double* __restrict__ xu,
                             const double* __restrict__ xv, const double* __restrict__ rhs_u,
                             const double* __restrict__ rhs_v, const double* __restrict__ phi, double* ru, double* rv,
                             double* dinv_u, double* dinv_v, CGScal* cg, RedSlot rs, int* iters_out,
                             cudaGraphConditionalHandle cond) {
-    __shared__ double sh[64];
+    __shared__ double sh[96];
     const int Nx = P.g.Nx;
     const double alpha = ac.value();
-    double acc[2] = {0.0, 0.0};
+    double acc[3] = {0.0, 0.0, 0.0};
     for_tiles(Nx, P.g.Ny, [&](int i, int j) {
         MuField mu = make_mu(P, phi);
         CompactUV x{xu, xv, Nx};
@@ -129,19 +148,16 @@ __global__ void k_visc_init(Params P, DtCoef ac, double reltol, int maxiter, con
         dinv_v[k] = d2;
         acc[0] += r1 * r1 + r2 * r2;
         acc[1] += r1 * r1 * d1 + r2 * r2 * d2;
+        // |b|^2 of the reference's row-eliminated system: Dirichlet rows carry their data
+        const double b1 = u_fixed(P, i) ? xu[k] : rhs_u[k], b2 = v_fixed(P, j) ? xv[k] : rhs_v[k];
+        acc[2] += b1 * b1 + b2 * b2;
     });
-    double tot[2];
-    if (grid_reduce<2>(acc, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0) {
+    double tot[3];
+    if (grid_reduce<3>(acc, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0) {
         cg->rr0 = tot[0];
         cg->rr = tot[0];
         cg->rz = tot[1];  // gamma_0 = r.M r
-        cg->tol2 = reltol * reltol * tot[0];
-        cg->iter = 0;
-        cg->maxiter = maxiter;
-        cg->alpha = 0.0;
-        cg->beta = 0.0;
-        cg->conv = tot[0] == 0.0 ? 1 : 0;
-        cg->done = (cg->conv || !isfinite(tot[0])) ? 1 : 0;  // a non-finite start ends at once
+        cg_begin(cg, o, tot[0], tot[2]);
         if (iters_out) *iters_out = 0;
         set_loop(cond, !cg->done);
     }
@@ -413,7 +429,7 @@ __global__ void __launch_bounds__(VTX * VTY, 4) k_visc_cg(Params P, DtCoef ac, c
         cg->rz = g;
         cg->pAp = d;
         if (tot[2] <= cg->tol2) { cg->conv = 1; cg->done = 1; }
-        else if (cg->iter >= cg->maxiter || !isfinite(tot[2])) cg->done = 1;
+        else if (cg->iter >= cg->maxiter || !isfinite(tot[2])) cg_unconverged(cg, tot[2]);
         if (iters_out) *iters_out = cg->iter;
         set_loop(cond, !cg->done);
     }
@@ -426,13 +442,13 @@ static ViscIterArgs visc_args(const ViscSolve& w, int parity) {
                         w.x_u, w.x_v, w.p_u, w.p_v, w.dinv_u, w.dinv_v};
 }
 
-void visc_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const double* Un, const double* Vn,
+void visc_init(const Params& P, DtCoef alpha, const SolveOpts& o, const double* Un, const double* Vn,
                const double* rhs_u, const double* rhs_v, const double* phi, const ViscSolve& w, CGScal* cg,
                const RedSlot& rs, const RedSlot& rs2, int* iters_out, cudaGraphConditionalHandle cond,
                cudaStream_t s) {
     dim3 g = grid2(P.g.Nx, P.g.Ny), b(BX, BY);
     k_visc_x0<<<g, b, 0, s>>>(P, Un, Vn, w.x_u, w.x_v);
-    k_visc_init<<<persistent_grid(tiles2(P.g.Nx, P.g.Ny), P.nsm, 2), b, 0, s>>>(P, alpha, reltol, maxiter, w.x_u, w.x_v, rhs_u, rhs_v, phi, w.r_u[0], w.r_v[0],
+    k_visc_init<<<persistent_grid(tiles2(P.g.Nx, P.g.Ny), P.nsm, 2), b, 0, s>>>(P, alpha, o, w.x_u, w.x_v, rhs_u, rhs_v, phi, w.r_u[0], w.r_v[0],
                                 w.dinv_u, w.dinv_v, cg, rs, iters_out, cond);
     // w_0 goes to the parity-0 "read" slot: the first iteration reads (r, w)[0].
     ViscIterArgs v = visc_args(w, 1);
@@ -503,7 +519,7 @@ __device__ __forceinline__ void visc_mx_slot(const Params& P, const ViscMxArgs& 
 //   REFINE   r = rhs - (I - alpha A) x in FP64; stop, or restart from it
 //   RESTART  w = A M r, r.Mr, Mr.w, from the refined residual
 template <bool START>
-__global__ void __launch_bounds__(VTX * VTY, 3) k_visc_mx(Params P, DtCoef ac, double reltol, int maxiter,
+__global__ void __launch_bounds__(VTX * VTY, 3) k_visc_mx(Params P, DtCoef ac, SolveOpts o,
                                                           const double* __restrict__ phi, ViscMxArgs v, CGScal* cg,
                                                           RedSlot rs, int* iters_out,
                                                           cudaGraphConditionalHandle cond) {
@@ -601,6 +617,10 @@ __global__ void __launch_bounds__(VTX * VTY, 3) k_visc_mx(Params P, DtCoef ac, d
                 v.rR_u[k] = (float)r1;
                 v.rR_v[k] = (float)r2;
                 acc[0] += r1 * r1 + r2 * r2;
+                if (START) {  // |b|^2 of the row-eliminated system (acc[1] is free at START)
+                    const double b1 = u_fixed(P, i) ? un : v.rhs_u[k], b2 = v_fixed(P, j) ? vn : v.rhs_v[k];
+                    acc[1] += b1 * b1 + b2 * b2;
+                }
             } else {
                 const double w1 = u_fixed(P, i) ? 0.0 : un - alpha * au;
                 const double w2 = v_fixed(P, j) ? 0.0 : vn - alpha * av;
@@ -622,15 +642,9 @@ __global__ void __launch_bounds__(VTX * VTY, 3) k_visc_mx(Params P, DtCoef ac, d
         if (START) {
             cg->rr0 = tot[0];
             cg->rr = tot[0];
-            cg->tol2 = reltol * reltol * tot[0];
-            cg->iter = 0;
-            cg->maxiter = maxiter;
-            cg->alpha = 0.0;
-            cg->beta = 0.0;
+            cg_begin(cg, o, tot[0], tot[1]);
             cg->inner = 0;
             cg->rr_restart = tot[0];
-            cg->conv = tot[0] == 0.0 ? 1 : 0;
-            cg->done = (cg->conv || !isfinite(tot[0])) ? 1 : 0;
             cg->phase = MX_RESTART;
             if (iters_out) *iters_out = 0;
             set_loop(cond, !cg->done);
@@ -646,12 +660,13 @@ __global__ void __launch_bounds__(VTX * VTY, 3) k_visc_mx(Params P, DtCoef ac, d
             cg->rz = g;
             cg->pAp = d;
             cg->inner += 1;
-            if (!isfinite(tot[2])) cg->done = 1;
+            cg->rr = tot[2];
+            if (!isfinite(tot[2])) cg_unconverged(cg, tot[2]);
             else if (tot[2] <= cg->tol2 || tot[2] <= kMxInnerDrop2 * cg->rr_restart) cg->phase = MX_REFINE;
         } else if (phase == MX_REFINE) {
             cg->rr = tot[0];
             if (tot[0] <= cg->tol2) { cg->conv = 1; cg->done = 1; }
-            else if (!isfinite(tot[0])) cg->done = 1;
+            else if (!isfinite(tot[0])) cg_unconverged(cg, tot[0]);
             else { cg->phase = MX_RESTART; cg->rr_restart = tot[0]; }
         } else {  // restart: r.Mr and Mr.w of the refined residual
             cg->rz = tot[0];
@@ -661,7 +676,7 @@ __global__ void __launch_bounds__(VTX * VTY, 3) k_visc_mx(Params P, DtCoef ac, d
             cg->inner = 0;
             cg->phase = MX_ITER;
         }
-        if (!cg->done && cg->iter >= cg->maxiter) cg->done = 1;
+        if (!cg->done && cg->iter >= cg->maxiter) cg_unconverged(cg, cg->rr);
         if (iters_out) *iters_out = cg->iter;
         set_loop(cond, !cg->done);
     }
@@ -675,14 +690,14 @@ static ViscMxArgs visc_mx_args(const ViscSolve& w, const ViscMixed& m, const dou
                       m.p_u, m.p_v, m.dinv_u, m.dinv_v, m.rR_u, m.rR_v, w.x_u, w.x_v, rhs_u, rhs_v};
 }
 
-void visc_mx_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const double* Un, const double* Vn,
+void visc_mx_init(const Params& P, DtCoef alpha, const SolveOpts& o, const double* Un, const double* Vn,
                   const double* rhs_u, const double* rhs_v, const double* phi, const ViscSolve& w,
                   const ViscMixed& m, CGScal* cg, const RedSlot& rs, int* iters_out,
                   cudaGraphConditionalHandle cond, cudaStream_t s) {
     k_visc_x0<<<grid2(P.g.Nx, P.g.Ny), dim3(BX, BY), 0, s>>>(P, Un, Vn, w.x_u, w.x_v);
     const int nt = ((P.g.Nx + VTX - 1) / VTX) * ((P.g.Ny + VTY - 1) / VTY);
     k_visc_mx<true><<<persistent_grid(nt, P.nsm, 3), dim3(VTX, VTY), 0, s>>>(
-        P, alpha, reltol, maxiter, phi, visc_mx_args(w, m, rhs_u, rhs_v, 0), cg, rs, iters_out, cond);
+        P, alpha, o, phi, visc_mx_args(w, m, rhs_u, rhs_v, 0), cg, rs, iters_out, cond);
 }
 
 void visc_mx_iter(const Params& P, DtCoef alpha, const double* phi, const double* rhs_u, const double* rhs_v,
@@ -690,7 +705,7 @@ void visc_mx_iter(const Params& P, DtCoef alpha, const double* phi, const double
                   int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s) {
     const int nt = ((P.g.Nx + VTX - 1) / VTX) * ((P.g.Ny + VTY - 1) / VTY);
     k_visc_mx<false><<<persistent_grid(nt, P.nsm, 3), dim3(VTX, VTY), 0, s>>>(
-        P, alpha, 0.0, 0, phi, visc_mx_args(w, m, rhs_u, rhs_v, parity), cg, rs, iters_out, cond);
+        P, alpha, SolveOpts{}, phi, visc_mx_args(w, m, rhs_u, rhs_v, parity), cg, rs, iters_out, cond);
 }
 
 // NoViscosity: predictor = rhs with the Dirichlet rows enforced (:786-788).
@@ -767,14 +782,14 @@ __device__ void diff_L(const Params& P, const double* phi, const F& f, int i, in
     diag = -(dx[0] + dx[1]) * ihx - (dy[0] + dy[1]) * ihy;
 }
 
-__global__ void k_diff_init(Params P, DtCoef ac, double reltol, int maxiter, const double* __restrict__ c0,
+__global__ void k_diff_init(Params P, DtCoef ac, SolveOpts o, const double* __restrict__ c0,
                             const double* __restrict__ rhs, const double* __restrict__ phi, double* x, double* r,
                             double* dinv, CGScal* cg, RedSlot rs, int* iters_out, cudaGraphConditionalHandle cond) {
-    __shared__ double sh[64];
+    __shared__ double sh[96];
     const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
     const int Nx = P.g.Nx;
     const double alpha = ac.value();
-    double acc[2] = {0.0, 0.0};
+    double acc[3] = {0.0, 0.0, 0.0};
     if (i < Nx && j < P.g.Ny) {
         auto f = [&](int a, int b) { return c0[cidx(a, b, Nx)]; };
         double L, d;
@@ -787,14 +802,12 @@ __global__ void k_diff_init(Params P, DtCoef ac, double reltol, int maxiter, con
         dinv[k] = di;
         acc[0] = rr * rr;
         acc[1] = rr * rr * di;
+        acc[2] = rhs[k] * rhs[k];
     }
-    double tot[2];
-    if (grid_reduce<2>(acc, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0) {
+    double tot[3];
+    if (grid_reduce<3>(acc, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0) {
         cg->rr0 = tot[0]; cg->rr = tot[0]; cg->rz = tot[1];
-        cg->tol2 = reltol * reltol * tot[0];
-        cg->iter = 0; cg->maxiter = maxiter; cg->beta = 0.0;
-        cg->conv = tot[0] == 0.0 ? 1 : 0;
-        cg->done = (cg->conv || !isfinite(tot[0])) ? 1 : 0;  // a non-finite start ends at once
+        cg_begin(cg, o, tot[0], tot[2]);
         if (iters_out) *iters_out = 0;
         set_loop(cond, !cg->done);
     }
@@ -859,16 +872,16 @@ __global__ void k_diff_update(Params P, const double* __restrict__ dinv, double*
         cg->beta = cg->rz != 0.0 ? tot[1] / cg->rz : 0.0;
         cg->rz = tot[1];
         if (tot[0] <= cg->tol2) { cg->conv = 1; cg->done = 1; }
-        else if (cg->iter >= cg->maxiter || !isfinite(tot[0])) cg->done = 1;
+        else if (cg->iter >= cg->maxiter || !isfinite(tot[0])) cg_unconverged(cg, tot[0]);
         if (iters_out) *iters_out = cg->iter;
         set_loop(cond, !cg->done);
     }
 }
 
-void diff_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const double* c0, const double* rhs,
+void diff_init(const Params& P, DtCoef alpha, const SolveOpts& o, const double* c0, const double* rhs,
                const double* phi, const ScalarSolve& w, CGScal* cg, const RedSlot& rs, int* iters_out,
                cudaGraphConditionalHandle cond, cudaStream_t s) {
-    k_diff_init<<<grid2(P.g.Nx, P.g.Ny), dim3(BX, BY), 0, s>>>(P, alpha, reltol, maxiter, c0, rhs, phi, w.x, w.r,
+    k_diff_init<<<grid2(P.g.Nx, P.g.Ny), dim3(BX, BY), 0, s>>>(P, alpha, o, c0, rhs, phi, w.x, w.r,
                                                               w.dinv, cg, rs, iters_out, cond);
 }
 void diff_iter(const Params& P, DtCoef alpha, const double* phi, const ScalarSolve& w, CGScal* cg, const RedSlot& rs1,
@@ -878,6 +891,24 @@ void diff_iter(const Params& P, DtCoef alpha, const double* phi, const ScalarSol
     k_diff_pupdate<<<std::min((n + 255) / 256, 148 * 8), 256, 0, s>>>(n, w.r, w.dinv, w.p[0], cg);
     k_diff_matvec<<<g, b, 0, s>>>(P, alpha, phi, w.p[0], w.Ap, cg, rs1);
     k_diff_update<<<g, b, 0, s>>>(P, w.dinv, w.x, w.r, w.p[0], w.Ap, cg, rs2, iters_out, cond);
+}
+
+// ---- judgement of a finished velocity / resource solve ----------------------------------
+SolveOpts solve_opts(const efsi_numerics& nu, int method) {
+    SolveOpts o;
+    const bool direct = method != EFSI_LINEAR_GMRES;
+    o.reltol = direct ? kDirectReltol : nu.linear_reltol;
+    o.maxiter = direct ? EFSI_LINEAR_HARD_CAP : std::max(1, nu.linear_maxiter);
+    o.fallback = (!direct && nu.direct_fallback) ? 1 : 0;  // DIRECT has nothing to fall back to
+    o.fb_tol = nu.fallback_reltol;
+    return o;
+}
+
+__global__ void k_solve_status(const CGScal* cg, DevStatus* st, int which, int stage) {
+    if (cg->fail) raise_err(st, DE_LINEAR_NOCONV, which, stage, cg->iter, cg->fail_rel);
+}
+void solve_status(const CGScal* cg, DevStatus* st, int which, int stage, cudaStream_t s) {
+    k_solve_status<<<1, 1, 0, s>>>(cg, st, which, stage);
 }
 
 // =====================================================================================

@@ -14,7 +14,50 @@ struct CGScal {
     // restart, squared residual at that restart
     int phase, inner;
     double rr_restart;
+    // judgement of a solve that stops short of its tolerance, as _solve_linear_system!
+    // judges a GMRES result (TimeIntegrationIMEX.jl:602-641): |b|^2 of the whole system
+    // (Dirichlet rows hold their data), fallback_reltol, whether the DIRECT continuation
+    // is allowed / running, and the outcome (fail: relative residual fail_rel too large)
+    double bnorm2, fb_tol, fail_rel;
+    int fallback, in_fallback, fail, pad;
 };
+
+// Tolerance and iteration limit of one velocity or resource solve, from its method
+// (EFSI_LINEAR_DIRECT: 1e-13 and EFSI_LINEAR_HARD_CAP; EFSI_LINEAR_GMRES: reltol and
+// maxiter) and the fallback options.
+struct SolveOpts {
+    double reltol;
+    int maxiter;
+    int fallback;
+    double fb_tol;
+};
+SolveOpts solve_opts(const efsi_numerics& nu, int method);
+
+// Squared relative residual of the DIRECT stand-in (1e-13 against the initial residual).
+constexpr double kDirectReltol = 1e-13;
+
+// The deciding thread of a velocity or resource CG calls this when the iteration
+// stops without meeting its tolerance (iteration limit or a non-finite residual;
+// rr = squared residual of the current iterate).  A relative residual within
+// fallback_reltol is accepted, as the reference accepts such a GMRES result;
+// otherwise the DIRECT continuation starts when allowed, or the solve fails.
+__device__ __forceinline__ void cg_unconverged(CGScal* cg, double rr) {
+    const double rel = sqrt(rr) / fmax(sqrt(cg->bnorm2), 2.220446049250313e-16);
+    if (isfinite(rel) && rel <= cg->fb_tol) { cg->done = 1; return; }
+    if (cg->fallback && !cg->in_fallback && isfinite(rel)) {
+        cg->in_fallback = 1;
+        cg->tol2 = kDirectReltol * kDirectReltol * cg->rr0;
+        cg->maxiter = cg->iter + EFSI_LINEAR_HARD_CAP;
+        return;
+    }
+    cg->done = 1;
+    cg->fail = 1;
+    cg->fail_rel = rel;
+}
+
+// Raise DE_LINEAR_NOCONV (EFSI_SOLVE) when the solve just finished failed its
+// judgement; `which` 0 = velocity, 1 = resource; `stage` the 0-based stage.
+void solve_status(const CGScal* cg, DevStatus* st, int which, int stage, cudaStream_t s);
 
 // ---- viscous predictor (I - alpha*A) u = rhs with Dirichlet rows eliminated --------
 // Chronopoulos-Gear (single-reduction) Jacobi-PCG: one kernel per iteration.  r, w
@@ -24,7 +67,7 @@ struct ViscSolve {
     double *x_u, *x_v, *p_u, *p_v, *dinv_u, *dinv_v;
     double *r_u[2], *r_v[2], *w_u[2], *w_v[2], *s_u[2], *s_v[2];
 };
-void visc_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const double* Un, const double* Vn,
+void visc_init(const Params& P, DtCoef alpha, const SolveOpts& o, const double* Un, const double* Vn,
                const double* rhs_u, const double* rhs_v, const double* phi, const ViscSolve& w, CGScal* cg,
                const RedSlot& rs, const RedSlot& rs2, int* iters_out, cudaGraphConditionalHandle cond,
                cudaStream_t s);
@@ -39,7 +82,7 @@ struct ViscMixed {
     float *r_u[2], *r_v[2], *w_u[2], *w_v[2], *s_u[2], *s_v[2];
     float *p_u, *p_v, *dinv_u, *dinv_v, *rR_u, *rR_v;
 };
-void visc_mx_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const double* Un, const double* Vn,
+void visc_mx_init(const Params& P, DtCoef alpha, const SolveOpts& o, const double* Un, const double* Vn,
                   const double* rhs_u, const double* rhs_v, const double* phi, const ViscSolve& w,
                   const ViscMixed& m, CGScal* cg, const RedSlot& rs, int* iters_out,
                   cudaGraphConditionalHandle cond, cudaStream_t s);
@@ -53,7 +96,7 @@ void visc_enforce_dirichlet(const Params& P, const double* rhs_u, const double* 
 struct ScalarSolve {
     double *x, *r, *p[2], *Ap, *dinv;
 };
-void diff_init(const Params& P, DtCoef alpha, double reltol, int maxiter, const double* c0, const double* rhs,
+void diff_init(const Params& P, DtCoef alpha, const SolveOpts& o, const double* c0, const double* rhs,
                const double* phi, const ScalarSolve& w, CGScal* cg, const RedSlot& rs, int* iters_out,
                cudaGraphConditionalHandle cond, cudaStream_t s);
 void diff_iter(const Params& P, DtCoef alpha, const double* phi, const ScalarSolve& w, CGScal* cg, const RedSlot& rs1,

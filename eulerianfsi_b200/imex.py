@@ -240,7 +240,7 @@ class Handle:
                 "resource_iterations": list(s.resource_iterations),
                 "kernel_launches": int(s.kernel_launches), "device_ms": float(s.device_ms),
                 "site_launches": int(s.site_launches), "site_ms": float(s.site_ms),
-                "site_bytes": float(s.site_bytes)}
+                "site_bytes": float(s.site_bytes), "step_bytes": float(s.step_bytes)}
 
 
 @dataclass

@@ -412,8 +412,13 @@ class FourStageIMEXFractionalStep:
 class LinearSolverOptions:
     """LinearSolverOptions (TimeIntegrationIMEX.jl:211-252).  On the device every
     implicit system is SPD after symmetric Dirichlet elimination and is solved by
-    preconditioned CG: `:direct` maps to a relative residual of 1e-13 (the exact
-    solution within round-off), `:gmres` to `reltol`."""
+    preconditioned CG, each system with its own method: `:direct` maps to a relative
+    residual of 1e-13 (the exact solution within round-off, at most
+    EFSI_LINEAR_HARD_CAP iterations), `:gmres` to `reltol` and `maxiter`.  The
+    result is then judged as _solve_linear_system! judges it (:602-641): a relative
+    residual |A x - b| / max(|b|, eps) that is non-finite or above `fallback_reltol`
+    continues with the `:direct` iteration when `direct_fallback` is set and
+    otherwise raises SolverError (the reference's ErrorException)."""
     velocity_method: str = "direct"
     resource_method: str = "gmres"
     reltol: float = 1e-8
@@ -437,8 +442,6 @@ class LinearSolverOptions:
         if not self.fallback_reltol > 0:
             raise ArgumentError("fallback_reltol must be positive.")
 
-
-DIRECT_RELTOL = 1e-13
 
 
 @dataclass(frozen=True)
@@ -598,6 +601,11 @@ def fill_numerics(out: _abi.Numerics, n: IMEXNumerics) -> None:
     out.stage1_constraint_rtol = n.stage1_constraint_rtol
     out.check_stage1_constraint = int(bool(n.check_stage1_constraint))
     ls = n.linear_solvers
-    out.linear_reltol = DIRECT_RELTOL if ls.velocity_method == "direct" else ls.reltol
+    method = {"direct": _abi.LINEAR_DIRECT, "gmres": _abi.LINEAR_GMRES}
+    out.velocity_method = method[ls.velocity_method]
+    out.resource_method = method[ls.resource_method]
+    out.linear_reltol = ls.reltol
     out.linear_maxiter = int(ls.maxiter)
+    out.direct_fallback = int(bool(ls.direct_fallback))
+    out.fallback_reltol = ls.fallback_reltol
     out.precision = _abi.PRECISION_MIXED if n.precision == "mixed" else _abi.PRECISION_FP64

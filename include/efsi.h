@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define EFSI_ABI_VERSION 1
+#define EFSI_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define EFSI_API __attribute__((visibility("default")))
@@ -153,14 +153,32 @@ typedef struct efsi_models {
 #define EFSI_PRECISION_MIXED        1   /* FP32 stencil bulk and multigrid, FP64 state, residuals,
                                            inner products, refinement and mass sums               */
 
+/* LinearSolverOptions.velocity_method / resource_method (TimeIntegrationIMEX.jl:211-233).
+ * Every implicit system is SPD after symmetric Dirichlet elimination and is solved by
+ * preconditioned CG on the device:
+ *   DIRECT  the stand-in for `A \ b`: relative residual 1e-13 (against the initial
+ *           residual), at most EFSI_LINEAR_HARD_CAP iterations;
+ *   GMRES   `reltol` and `maxiter` of the options.
+ * After either, the relative residual |A x - b| / max(|b|, eps) decides as in
+ * _solve_linear_system! (:602-641): non-finite or above fallback_reltol falls back
+ * to the DIRECT iteration (up to EFSI_LINEAR_HARD_CAP more iterations) when
+ * direct_fallback is set, and otherwise fails the step with EFSI_SOLVE. */
+#define EFSI_LINEAR_DIRECT          0
+#define EFSI_LINEAR_GMRES           1
+#define EFSI_LINEAR_HARD_CAP        10000
+
 typedef struct efsi_numerics {
     int32_t structure_extension;  double extension_rate, extension_exponent, extension_cutoff;
     double  projection_reltol;    int32_t projection_maxiter;
     double  stage1_constraint_atol, stage1_constraint_rtol;
     int32_t check_stage1_constraint;
-    double  linear_reltol;        int32_t linear_maxiter;    /* velocity and resource solves */
+    double  linear_reltol;        int32_t linear_maxiter;    /* options.reltol, options.maxiter */
     int32_t precision;            /* EFSI_PRECISION_*                                          */
-    int32_t reserved[7];
+    int32_t velocity_method;      /* EFSI_LINEAR_*                                             */
+    int32_t resource_method;      /* EFSI_LINEAR_*                                             */
+    int32_t direct_fallback;      /* options.direct_fallback                                   */
+    double  fallback_reltol;      /* options.fallback_reltol                                   */
+    int32_t reserved[4];
 } efsi_numerics;
 
 typedef struct efsi_config {
@@ -223,6 +241,8 @@ typedef struct efsi_stats {
     double  site_ms;                    /* their summed CUDA-event duration               */
     double  site_bytes;                 /* their summed algorithmic bytes (unique reads +
                                            writes once, FP64)                            */
+    double  step_bytes;                 /* summed algorithmic bytes of every site launch of
+                                           host-driven steps since efsi_set_timed_site    */
 } efsi_stats;
 
 /* Driver diagnostics of the cavity benchmarks (run_sugiyama_lid_driven_cavity.jl),
@@ -364,6 +384,17 @@ EFSI_API int efsi_state_diagnostics(efsi_handle* h, const efsi_diag_config* conf
  * efsi_stats.  Tracing aid of the benchmark; no reference counterpart. */
 EFSI_API int efsi_set_timed_site(efsi_handle* h, int32_t site);
 
+/* How efsi_integrate_step / efsi_integrate_step_host / efsi_step_n run a step:
+ *   EFSI_STEP_GRAPH  (default) the whole step is one captured CUDA graph whose
+ *                    solver loops are device-terminated conditional nodes;
+ *   EFSI_STEP_HOST   every kernel is an ordinary launch from the host, the solver
+ *                    loops enqueued in batches (for profilers that list launches).
+ * Both run the same kernels and give bit-identical states.  No reference
+ * counterpart (the reference has no device). */
+#define EFSI_STEP_GRAPH 0
+#define EFSI_STEP_HOST  1
+EFSI_API int efsi_set_step_mode(efsi_handle* h, int32_t mode);
+
 /* Allocation-free check of a MAC velocity against a divergence target: writes
  * out[0] = max |div(U,V) - G| and out[1] = max |G| over the Nx x Ny cells of a
  * uniform grid on [0,Lx] x [0,Ly] (G may be NULL for a zero target; the same
@@ -374,6 +405,8 @@ EFSI_API int efsi_set_timed_site(efsi_handle* h, int32_t site);
  * cudaMalloc/cudaFree may cause.  It needs no handle, calls no allocator, and works
  * directly on the caller's device arrays (U (Nx+1) x Ny, V Nx x (Ny+1), G and out
  * on the current device).
+ *  - A cell whose residual (or |G|) is not finite (NaN or Inf anywhere in its
+ *    stencil) makes out[0] (or out[1]) +Inf, so a corrupt field never passes.
  *  - Asynchronous: the kernel runs on `stream` (a cudaStream_t; NULL is the legacy
  *    default stream); out is valid once that stream has been synchronised.
  *  - Scratch: a fixed 256 KiB static device array inside the library holds the

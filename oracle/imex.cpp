@@ -5,6 +5,7 @@
 // drive the oracle and the CUDA library with the same host code.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <functional>
 #include <memory>
@@ -83,9 +84,36 @@ static void validate_state(const Ctx& C, const F2& U, const F2& V, const F2& phi
     (void)C;
 }
 
+// _solve_linear_system! (TimeIntegrationIMEX.jl:602-641) with BiCGStab standing in for
+// both methods: :direct is a 1e-13 solve; :gmres runs to reltol within maxiter and
+// is judged by |A x - b| / max(|b|, eps): non-finite or above fallback_reltol falls
+// back to the 1e-13 solve when direct_fallback is set and throws otherwise (:637).
+static int judged_solve(const OpFn& op, const std::vector<double>& b, std::vector<double>& x, int method,
+                        const efsi_numerics& nu, const std::string& name) {
+    if (method != EFSI_LINEAR_GMRES) return bicgstab(op, b, x, 1e-13, EFSI_LINEAR_HARD_CAP);
+    int it = bicgstab(op, b, x, nu.linear_reltol, std::max(nu.linear_maxiter, 1));
+    std::vector<double> ax;
+    op(x, ax);
+    double rn = 0.0, bn = 0.0;
+    for (size_t k = 0; k < b.size(); ++k) {
+        rn += (ax[k] - b[k]) * (ax[k] - b[k]);
+        bn += b[k] * b[k];
+    }
+    const double rr = std::sqrt(rn) / std::max(std::sqrt(bn), 2.220446049250313e-16);
+    if (!std::isfinite(rr) || rr > nu.fallback_reltol) {
+        if (!nu.direct_fallback) {
+            char buf[64];
+            snprintf(buf, sizeof buf, "%.17g", rr);
+            solve_error(name + " GMRES residual is too large: " + buf);
+        }
+        it += bicgstab(op, b, x, 1e-13, EFSI_LINEAR_HARD_CAP);
+    }
+    return it;
+}
+
 // Solve (I - alpha*A) x = rhs with the reference's row Dirichlet elimination (:643-672, :786-812).
 static void velocity_solve(const Ctx& C, const F2& mu, double alpha, std::vector<double>& rhs,
-                           std::vector<double>& x, int& iters) {
+                           std::vector<double>& x, int& iters, int stage) {
     std::vector<int> idx;
     std::vector<double> val;
     velocity_dirichlet_data(C.m, C.bu, C.bv, idx, val);
@@ -97,11 +125,11 @@ static void velocity_solve(const Ctx& C, const F2& mu, double alpha, std::vector
         out.resize(in.size());
         for (size_t k = 0; k < in.size(); ++k) out[k] = fixed[k] ? in[k] : in[k] - alpha * ax[k];
     };
-    iters = bicgstab(op, rhs, x, C.nu.linear_reltol, std::max(C.nu.linear_maxiter, 1) * 10);
+    iters = judged_solve(op, rhs, x, C.nu.velocity_method, C.nu, "velocity stage " + std::to_string(stage + 1));
 }
 
 static void resource_solve(const Ctx& C, const F2& D, double alpha, const std::vector<double>& rhs,
-                           std::vector<double>& x, int& iters) {
+                           std::vector<double>& x, int& iters, int stage) {
     OpFn op = [&](const std::vector<double>& in, std::vector<double>& out) {
         F2 f(C.m.Nx, C.m.Ny);
         f.a = in;
@@ -110,7 +138,7 @@ static void resource_solve(const Ctx& C, const F2& D, double alpha, const std::v
         out.resize(in.size());
         for (size_t k = 0; k < in.size(); ++k) out[k] = in[k] - alpha * Lf.a[k];
     };
-    iters = bicgstab(op, rhs, x, C.nu.linear_reltol, std::max(C.nu.linear_maxiter, 1) * 10);
+    iters = judged_solve(op, rhs, x, C.nu.resource_method, C.nu, "resource stage " + std::to_string(stage + 1));
 }
 
 struct Tend {
@@ -249,7 +277,7 @@ static void integrate_step(Ctx& C, double t, double dt, efsi_step_report* rep) {
                 for (size_t k = 0; k < N; ++k) rc[k] += alpha * bD.a[k];
                 std::vector<double> x = cn.a;
                 int it = 0;
-                resource_solve(C, D, alpha, rc, x, it);
+                resource_solve(C, D, alpha, rc, x, it, s);
                 C.stats.resource_iterations[s] = it;
                 cs.a = x;
             }
@@ -295,7 +323,7 @@ static void integrate_step(Ctx& C, double t, double dt, efsi_step_report* rep) {
                 for (size_t k = 0; k < 2 * N; ++k) rhs[k] += alpha * bvis[k];
                 pred = uvn;
                 int it = 0;
-                velocity_solve(C, mu, alpha, rhs, pred, it);
+                velocity_solve(C, mu, alpha, rhs, pred, it, s);
                 C.stats.velocity_iterations[s] = it;
             }
             inject(Us, Vs, pred, C);

@@ -59,11 +59,20 @@ def test_full_size_properties_over_twenty_steps(precision):
     area = np.outer(w.metrics.dx_c, w.metrics.dy_c)
     m0, m1 = float(np.sum(w.state.phi * area)), float(np.sum(st.phi * area))
     assert abs(m1 - m0) <= 1e-12 * m0, (m0, m1)
+    # The bound is the reference's own acceptance test of a projected velocity: the
+    # stage-1 check of the next step (TimeIntegrationIMEX.jl:1111-1127) rejects
+    # max |div v - G| above atol + rtol * max(max|G|, 1) (5e-8 + 1e-8 here).
+    num = w.numerics
+    accept = num.stage1_constraint_atol + num.stage1_constraint_rtol
     for r in reps:
-        assert r.maximum_projection_constraint_linf <= 1e-6
+        assert r.maximum_projection_constraint_linf <= accept, r.maximum_projection_constraint_linf
         assert r.minimum_sigma_eigenvalue > 0.0 and r.non_spd_cells == 0
     for a in st.arrays():
         assert np.all(np.isfinite(a))
     hx = hy = 1.0 / 1024
     div = (st.U[1:, :] - st.U[:-1, :]) / hx + (st.V[:, 1:] - st.V[:, :-1]) / hy
-    assert float(np.max(np.abs(div))) <= 1e-6
+    # the host's divergence of the returned velocity is the constraint the step reported
+    # (to the rounding of the terms whose difference it is)
+    scale = float(np.max(np.abs(st.U))) / hx + float(np.max(np.abs(st.V))) / hy
+    assert float(np.max(np.abs(div))) <= reps[n - 1].maximum_projection_constraint_linf + 1e-12 * scale
+    assert float(np.max(np.abs(div))) <= accept

@@ -99,3 +99,22 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
                                               buf.data_ptr(), None)
     assert st == _abi.ARG
     assert b"fixed scratch" in lib.efsi_last_error(None)
+
+
+def test_noalloc_reports_non_finite_fields():
+    """A NaN or Inf in the velocity or the target never yields a finite residual (a
+    plain max reduction would drop a NaN and report the rest of the grid)."""
+    torch = pytest.importorskip("torch")
+    lib = _abi.load_library()
+    metrics, U, V, G, _ = _projected("dirichlet")
+    bad_U = U.copy(order="F")
+    bad_U[5, 7] = np.nan
+    got = _noalloc(lib, torch, metrics, bad_U, V, G)
+    assert not np.isfinite(got[0]) and np.isfinite(got[1])
+    bad_G = G.copy(order="F")
+    bad_G[3, 2] = np.inf
+    got = _noalloc(lib, torch, metrics, U, V, bad_G)
+    assert not np.isfinite(got[0]) and not np.isfinite(got[1])
+    # the same shared scratch still gives the finite answer afterwards
+    got = _noalloc(lib, torch, metrics, U, V, G)
+    assert np.isfinite(got[0]) and got[1] == float(np.max(np.abs(G)))
