@@ -118,6 +118,11 @@ class Stats(Structure):
                 ("site_bytes", c_double), ("step_bytes", c_double)]
 
 
+class GradientC(Structure):
+    _fields_ = [("elastic_coefficient", c_double), ("U_bottom", _dp), ("U_top", _dp), ("V_left", _dp),
+                ("V_right", _dp)]
+
+
 DIAG_MAX_MODES = 8
 
 
@@ -176,6 +181,10 @@ SIGNATURES = {
 CUDA_ONLY = {
     "set_timed_site": (c_int32, [_H, c_int32]),
     "set_step_mode": (c_int32, [_H, c_int32]),
+    "forward_checkpointed": (c_int32, [_H, c_double, _dp, c_int32, c_int32, POINTER(StepReportC)]),
+    "backward": (c_int32, [_H] + [_dp] * 12 + [c_void_p]),
+    "tendencies_adjoint": (c_int32, [_H] + [_dp] * 20 + [c_void_p]),
+    "project_adjoint": (c_int32, [_H] + [_dp] * 4),
     "integrate_step_host": (c_int32, [_H] + [_dp] * 8 + [c_double, c_double, POINTER(StepReportC)]),
     "step_n": (c_int32, [_H, c_double, _dp, c_int32, POINTER(StepReportC)]),
     # no handle: device pointers in, device result out (allocates nothing)

@@ -22,6 +22,7 @@
 #include <string>
 #include <vector>
 
+#include "efsi_adjoint.cuh"
 #include "efsi_diag.cuh"
 #include "efsi_kernels.cuh"
 #include "efsi_solvers.cuh"
@@ -108,14 +109,46 @@ struct efsi_handle {
     // solver batch predictions (host-driven mode)
     int pred[3] = {4, 4, 4};
     long long launches = 0;
-    // step graph: the whole IMEX step captured once, CG loops as WHILE nodes
+    // step graphs: the whole IMEX step captured once, CG loops as WHILE nodes; slot 1 is
+    // the same step with the tape records of the differentiation form
     cudaStream_t stream2 = nullptr;
     bool use_graph = true, capturing = false;
-    cudaGraph_t step_graph = nullptr;
-    cudaGraphExec_t step_exec = nullptr;
-    long long fixed_launches = 0;
     struct Loop { int kind, stage, kernels_per_body, iters_per_body; };
-    std::vector<Loop> loops;
+    struct GraphSlot {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        long long fixed_launches = 0;
+        std::vector<Loop> loops;
+    };
+    GraphSlot gs[2];
+    // differentiation form: the state every `adj_every` steps of the last
+    // efsi_forward_checkpointed call, the tape of one recomputed segment, and the
+    // adjoint buffers (allocated on first use)
+    bool recording = false;
+    int adj_n = 0, adj_every = 0, adj_ckpt_cap = 0, adj_tape_cap = 0;
+    double adj_t0 = 0.0;
+    std::vector<double> adj_dts;
+    double* ckpt = nullptr;         // adj_ckpt_cap slots of ckpt_stride()
+    double* tape = nullptr;         // adj_tape_cap slots of tape_stride()
+    double* adj = nullptr;          // adjoint buffers, see adjoint_buffers()
+    size_t adj_words = 0;
+    struct AdjBufs {
+        double *lU, *lV, *lphi, *lsxx, *lsyy, *lsxy;     // adjoint of the state (in and out of a reverse step)
+        double *sU, *sV, *sphi, *ssxx, *ssyy, *ssxy;     // adjoint of one stage's fields
+        double *acc;                                     // start of the block cleared per reverse step:
+        double *luu, *luv, *lphin, *lsxn, *lsyn, *lscn;  //   adjoint of uv_n, phi_n, sigma_n'
+        double *lEu[3], *lEv[3], *lIu[3], *lIv[3], *lEphi[3], *lExx[3], *lEyy[3], *lExy[3];  //   of histories
+        size_t acc_words;
+        double *lpu, *lpv;                               // adjoint of the predictor (compact)
+        double *zU, *zV, *zq;                            // zeros: starts of the adjoint solves
+        double *s0x, *s0y, *s0c;                         // sigma_n' of the step being reversed
+        double *final_state;                             // the state after the forward sweep (restored)
+        AdjScratch sc;
+        double *bub, *but, *bvl, *bvr, *G;               // parameter adjoints
+    } ab{};
+    size_t block_words() const { return nu + nv + 4 * nc; }            // U, V, phi, sigma x3
+    size_t tape_stride() const { return 3 * block_words() + nc; }      // start, stage 1, stage 2, phi_3
+    size_t ckpt_stride() const { return nu + nv + 6 * nc; }            // U, V, phi, c, sigma x3, q
     double* times_dev = nullptr;    // (t, dt) per step of a batch
     double* times_pinned = nullptr;
     StepRec* hist_dev = nullptr;
@@ -142,8 +175,11 @@ struct efsi_handle {
         for (auto& e : site_ev) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
         for (cudaEvent_t e : call_ev) if (e) cudaEventDestroy(e);
         for (void* p : allocs) cudaFree(p);
-        if (step_exec) cudaGraphExecDestroy(step_exec);
-        if (step_graph) cudaGraphDestroy(step_graph);
+        for (double* p : {ckpt, tape, adj}) if (p) cudaFree(p);
+        for (GraphSlot& g : gs) {
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            if (g.graph) cudaGraphDestroy(g.graph);
+        }
         if (host) cudaFreeHost(host);
         if (done_pinned) cudaFreeHost(done_pinned);
         if (times_pinned) cudaFreeHost(times_pinned);
@@ -616,7 +652,7 @@ void solve(efsi_handle* h, int kind, int stage, CGScal* cg, int maxiter, int ker
         body(h->stream2, iters_out, ch);
         cudaGraph_t out;
         check_cuda(cudaStreamEndCapture(h->stream2, &out), "body capture");
-        h->loops.push_back({kind, stage, kernels_per_body, iters_per_body});
+        h->gs[h->recording ? 1 : 0].loops.push_back({kind, stage, kernels_per_body, iters_per_body});
         return;
     }
     init(h->stream, iters_out, (cudaGraphConditionalHandle)0);
@@ -636,22 +672,19 @@ void solve(efsi_handle* h, int kind, int stage, CGScal* cg, int maxiter, int ker
     h->pred[kind] = std::max(1, flags[0]);
 }
 
-// One projection of (compact predictor | full arrays) onto div = G, writing U_out/V_out/q.
-void projection(efsi_handle* h, bool compact, const double* u_in, const double* v_in, const double* G, double* U_out,
-                double* V_out, int stage_slot) {
+// The Poisson solve K x = pj.b (MG-preconditioned CG) from the warm start q0.
+void proj_solve(efsi_handle* h, int stage_slot, double reltol, const double* q0) {
     const Params& P = h->P;
     DevBlock* d = h->dev;
-    const double N = (double)h->nc, nuv = (double)(h->nu + h->nv), g = G ? 1.0 : 0.0;
-    site(h, EFSI_SITE_PROJ_RHS, 8.0 * (2.0 * nuv + N * (2.0 + g)),
-         [&] { proj_rhs(P, h->pj, compact, u_in, v_in, G, &d->ps, h->slot[0], &d->st, h->stream); });
+    const double N = (double)h->nc;
     const double vb = proj_update_vcycle_bytes(h->pj);
     const int vk = proj_update_vcycle_kernels(h->pj);
     solve(
         h, KIND_PROJ, stage_slot, &d->cg_proj, P.nu.projection_maxiter,
         2 * (proj_matvec_kernels(h->pj) + vk), 2,
         [&](cudaStream_t s, int* io, cudaGraphConditionalHandle ch) {
-            proj_cg_init(P, h->pj, P.nu.projection_reltol, P.nu.projection_maxiter, h->q, &d->cg_proj, &d->ps,
-                         h->slot[1], h->slot[2], &d->st, io, ch, s);
+            proj_cg_init(P, h->pj, reltol, P.nu.projection_maxiter, q0, &d->cg_proj, &d->ps, h->slot[1],
+                         h->slot[2], &d->st, io, ch, s);
             h->launches += proj_init_kernels(h->pj);
         },
         [&](cudaStream_t s, int* io, cudaGraphConditionalHandle ch) {
@@ -663,6 +696,17 @@ void projection(efsi_handle* h, bool compact, const double* u_in, const double* 
                 });
             }
         });
+}
+
+// One projection of (compact predictor | full arrays) onto div = G, writing U_out/V_out/q.
+void projection(efsi_handle* h, bool compact, const double* u_in, const double* v_in, const double* G, double* U_out,
+                double* V_out, int stage_slot) {
+    const Params& P = h->P;
+    DevBlock* d = h->dev;
+    const double N = (double)h->nc, nuv = (double)(h->nu + h->nv), g = G ? 1.0 : 0.0;
+    site(h, EFSI_SITE_PROJ_RHS, 8.0 * (2.0 * nuv + N * (2.0 + g)),
+         [&] { proj_rhs(P, h->pj, compact, u_in, v_in, G, &d->ps, h->slot[0], &d->st, h->stream); });
+    proj_solve(h, stage_slot, P.nu.projection_reltol, h->q);
     site(h, EFSI_SITE_PROJ_FINISH, 8.0 * (4.0 * N + 2.0 * nuv + g * N), [&] {
         proj_finish(P, h->pj, G, h->q, U_out, V_out, &d->ps, &d->max_constraint, h->slot[6], h->slot[7], &d->st,
                     h->stream);
@@ -711,6 +755,10 @@ void enqueue_step(efsi_handle* h) {
     cudaStream_t s = h->stream;
     const double* dtp = &d->dt;
     k_begin_step<<<1, 1, 0, s>>>(d, h->times_dev);
+    if (h->recording) {  // tape slot of this step: the state it starts from
+        adj_record(P, &d->counter, h->tape_stride(), 0, h->U, h->V, h->phi, h->sxx, h->syy, h->sxy, h->tape, s);
+        h->launches += 1;
+    }
     launch_prepare_step(P, h->U, h->V, h->phi, h->c, h->sxx, h->syy, h->sxy, h->sxn, h->syn, h->sxyn, &d->st, s);
     h->launches += 2;
     const double* Gp = h->growth ? h->G : nullptr;
@@ -809,13 +857,25 @@ void enqueue_step(efsi_handle* h) {
             }
             projection(h, true, h->vs.x_u, h->vs.x_v, Gp, h->Us, h->Vs, st);
         }
-        if (st < 3) tendencies(h, st, f);
+        if (st < 3) {
+            if (h->recording && st > 0) {  // the stage fields the tendencies read
+                adj_record(P, &d->counter, h->tape_stride(), st * h->block_words(), h->Us, h->Vs, h->phis, h->sxs,
+                           h->sys, h->sxys, h->tape, s);
+                h->launches += 1;
+            }
+            tendencies(h, st, f);
+        }
     }
     site(h, EFSI_SITE_FINALIZE, 16.0 * (double)(h->nu + h->nv + 5 * h->nc), [&] {
         launch_finalize(P, h->Us, h->Vs, h->phis, h->resource ? h->cs : h->c, h->sxs, h->sys, h->sxys, h->U, h->V,
                         h->phi, h->c, h->sxx, h->syy, h->sxy, d->report, &d->nonspd, h->slot[0], h->slot[1], &d->st,
                         s);
     });
+    if (h->recording) {  // phi of the committed state (the last stage's extension mask)
+        adj_record(P, &d->counter, h->tape_stride(), 3 * h->block_words() - h->nu - h->nv, nullptr, nullptr, h->phi,
+                   nullptr, nullptr, nullptr, h->tape, s);
+        h->launches += 1;
+    }
     k_end_step<<<1, 1, 0, s>>>(d, h->hist_dev);
     h->launches += 2;
 }
@@ -824,9 +884,10 @@ void enqueue_step(efsi_handle* h) {
 // nodes).  If the driver refuses any part, the handle falls back to host-driven
 // stepping.
 void ensure_graph(efsi_handle* h) {
-    if (!h->use_graph || h->step_exec) return;
+    efsi_handle::GraphSlot& G = h->gs[h->recording ? 1 : 0];
+    if (!h->use_graph || G.exec) return;
     h->capturing = true;
-    h->loops.clear();
+    G.loops.clear();
     h->launches = 0;
     bool ok = true;
     try {
@@ -845,25 +906,26 @@ void ensure_graph(efsi_handle* h) {
         }
         cudaGraph_t g = nullptr;
         check_cuda(cudaStreamEndCapture(h->stream, &g), "capture");
-        h->step_graph = g;
-        check_cuda(cudaGraphInstantiate(&h->step_exec, g, 0), "graph instantiate");
+        G.graph = g;
+        check_cuda(cudaGraphInstantiate(&G.exec, g, 0), "graph instantiate");
     } catch (const Err&) {
         ok = false;
     }
     h->capturing = false;
-    h->fixed_launches = h->launches;
+    G.fixed_launches = h->launches;
     if (!ok) {
         cudaGetLastError();
-        if (h->step_exec) { cudaGraphExecDestroy(h->step_exec); h->step_exec = nullptr; }
-        if (h->step_graph) { cudaGraphDestroy(h->step_graph); h->step_graph = nullptr; }
+        if (G.exec) { cudaGraphExecDestroy(G.exec); G.exec = nullptr; }
+        if (G.graph) { cudaGraphDestroy(G.graph); G.graph = nullptr; }
         h->use_graph = false;
     }
 }
 
 // Kernel launches of the last graph step, from its recorded iteration counts.
 long long graph_launches(const efsi_handle* h, const StepRec& r) {
-    long long n = h->fixed_launches;
-    for (const auto& l : h->loops)  // a body runs whole; its later iterations return at once
+    const efsi_handle::GraphSlot& G = h->gs[h->recording ? 1 : 0];
+    long long n = G.fixed_launches;
+    for (const auto& l : G.loops)  // a body runs whole; its later iterations return at once
         n += (long long)((r.iters[l.kind][l.stage] + l.iters_per_body - 1) / l.iters_per_body) * l.kernels_per_body;
     return n;
 }
@@ -891,7 +953,8 @@ void run_steps(efsi_handle* h, double t0, const double* dts, int n, efsi_step_re
     } else {
         ensure_graph(h);
     }
-    const bool graph = h->use_graph && h->step_exec && h->timed_site == EFSI_SITE_NONE;
+    cudaGraphExec_t exec = h->gs[h->recording ? 1 : 0].exec;
+    const bool graph = h->use_graph && exec && h->timed_site == EFSI_SITE_NONE;
     long long launches = 0;
     int32_t its[3][4] = {};
     k_reset_call<<<1, 1, 0, h->stream>>>(h->dev);
@@ -911,7 +974,7 @@ void run_steps(efsi_handle* h, double t0, const double* dts, int n, efsi_step_re
         }
         for (int k = 0; k < m; ++k) {
             if (graph) {
-                check_cuda(cudaGraphLaunch(h->step_exec, h->stream), "graph launch");
+                check_cuda(cudaGraphLaunch(exec, h->stream), "graph launch");
             } else {
                 h->launches = 0;
                 enqueue_step(h);
@@ -942,6 +1005,165 @@ void run_steps(efsi_handle* h, double t0, const double* dts, int n, efsi_step_re
         h->stats.velocity_iterations[b] = its[KIND_VISC][b];
         h->stats.resource_iterations[b] = its[KIND_DIFF][b];
     }
+}
+
+// ---------------------------------------------------------------------------------------
+// differentiation form: sqrt(n) checkpoints, recomputed segments, reverse steps
+// ---------------------------------------------------------------------------------------
+constexpr double kAdjointReltol = 1e-13;  // the adjoint solves stand in for exact inverses
+
+__global__ void k_set_dt(DevBlock* d, double dt) { d->dt = dt; }
+
+void ensure_adjoint_buffers(efsi_handle* h) {
+    if (h->adj) return;
+    const size_t N = h->nc, nu = h->nu, nv = h->nv;
+    const size_t nbx = (size_t)h->Nx + 1, nby = (size_t)h->Ny + 1;
+    const size_t acc_words = 6 * N + 24 * N;
+    const size_t words = 2 * (nu + nv + 4 * N) + acc_words + 2 * N + (nu + nv + N) + 3 * N + h->ckpt_stride() +
+                         9 * N + 2 * nbx + 2 * nby + 1;
+    double* p = nullptr;
+    check_cuda(cudaMalloc(&p, words * sizeof(double)), "adjoint buffers");
+    check_cuda(cudaMemset(p, 0, words * sizeof(double)), "adjoint buffers");
+    h->adj = p;
+    h->adj_words = words;
+    efsi_handle::AdjBufs& a = h->ab;
+    auto take = [&](size_t n) { double* q = p; p += n; return q; };
+    a.lU = take(nu); a.lV = take(nv); a.lphi = take(N); a.lsxx = take(N); a.lsyy = take(N); a.lsxy = take(N);
+    a.sU = take(nu); a.sV = take(nv); a.sphi = take(N); a.ssxx = take(N); a.ssyy = take(N); a.ssxy = take(N);
+    a.acc = p;
+    a.acc_words = acc_words;
+    a.luu = take(N); a.luv = take(N); a.lphin = take(N); a.lsxn = take(N); a.lsyn = take(N); a.lscn = take(N);
+    for (int q = 0; q < 3; ++q) {
+        a.lEu[q] = take(N); a.lEv[q] = take(N); a.lIu[q] = take(N); a.lIv[q] = take(N);
+        a.lEphi[q] = take(N); a.lExx[q] = take(N); a.lEyy[q] = take(N); a.lExy[q] = take(N);
+    }
+    a.lpu = take(N); a.lpv = take(N);
+    a.zU = take(nu); a.zV = take(nv); a.zq = take(N);
+    a.s0x = take(N); a.s0y = take(N); a.s0c = take(N);
+    a.final_state = take(h->ckpt_stride());
+    a.sc = AdjScratch{take(N), take(N), take(N), take(N), take(N), take(N), take(N), take(N), take(N)};
+    a.bub = take(nbx); a.but = take(nbx); a.bvl = take(nby); a.bvr = take(nby); a.G = take(1);
+}
+
+// Copy the state and the warm start into (save) or out of (!save) a checkpoint slot.
+void state_copy(efsi_handle* h, double* slot, bool save) {
+    const size_t N = h->nc;
+    double* f[8] = {h->U, h->V, h->phi, h->c, h->sxx, h->syy, h->sxy, h->q};
+    const size_t n[8] = {h->nu, h->nv, N, N, N, N, N, N};
+    size_t off = 0;
+    for (int k = 0; k < 8; ++k) {
+        double* dst = save ? slot + off : f[k];
+        const double* src = save ? f[k] : slot + off;
+        check_cuda(cudaMemcpyAsync(dst, src, n[k] * sizeof(double), cudaMemcpyDeviceToDevice, h->stream), "checkpoint");
+        off += n[k];
+    }
+}
+
+void zero(efsi_handle* h, double* p, size_t n) {
+    check_cuda(cudaMemsetAsync(p, 0, n * sizeof(double), h->stream), "clear");
+}
+
+// Transposed projection of stage `st`: lam of the predictor (compact) from lam of the
+// projected face velocities.
+void adj_projection(efsi_handle* h, int st, const double* lU, const double* lV, double* lpu, double* lpv) {
+    const Params& P = h->P;
+    DevBlock* d = h->dev;
+    adj_proj_rhs(P, h->pj, lU, lV, &d->ps, h->slot[0], h->stream);
+    proj_solve(h, st, kAdjointReltol, h->ab.zq);
+    proj_mean(P, h->pj, &d->ps, h->slot[6], h->stream);
+    adj_proj_finish(P, h->pj, lU, lV, &d->ps, lpu, lpv, h->stream);
+    h->launches += 3;
+}
+
+// Transposed viscous solve of stage `st` (the free block of I - dt a_ss A is symmetric):
+// lam of the right-hand side in h->vs.x_u / x_v.
+void adj_viscous(efsi_handle* h, int st, const double* phis, const double* ru, const double* rv) {
+    const Params Ph = homogeneous(h->P);  // homogeneous Dirichlet rows: their data is not differentiated here
+    DevBlock* d = h->dev;
+    DtCoef alpha{&d->dt, c_AI_diag[st]};
+    SolveOpts o{kAdjointReltol, EFSI_LINEAR_HARD_CAP, 0, h->P.nu.fallback_reltol};
+    solve(
+        h, KIND_VISC, st, &d->cg_visc, o.maxiter, 2, 2,
+        [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
+            visc_init(Ph, alpha, o, h->ab.zU, h->ab.zV, ru, rv, phis, h->vs, &d->cg_visc, h->slot[0], h->slot[1], io,
+                      ch, ss);
+            h->launches += 3;
+        },
+        [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
+            for (int k = 0; k < 2; ++k) visc_iter(Ph, alpha, phis, h->vs, k, &d->cg_visc, h->slot[2], io, ch, ss);
+        });
+    solve_status(&d->cg_visc, &d->st, 0, st, h->stream);
+    h->launches += 1;
+}
+
+// One step backwards (TimeIntegrationIMEX.jl:1159-1255 in reverse) from the tape slot of
+// the step: ab.l* holds the adjoint of the state after the step on entry and the adjoint
+// of the state before it on return; parameter adjoints accumulate.
+void reverse_step(efsi_handle* h, int slot, double dt) {
+    const Params& P = h->P;
+    DevBlock* d = h->dev;
+    cudaStream_t s = h->stream;
+    efsi_handle::AdjBufs& a = h->ab;
+    const size_t N = h->nc, nu = h->nu, nv = h->nv, B = h->block_words();
+    const double* T = h->tape + (size_t)slot * h->tape_stride();
+    auto fields = [&](const double* b) {
+        return AdjIn{b, b + nu, b + nu + nv, b + nu + nv + N, b + nu + nv + 2 * N, b + nu + nv + 3 * N};
+    };
+    AdjIn f[3] = {fields(T), fields(T + B), fields(T + 2 * B)};
+    const double* phi3 = T + 3 * B;
+    k_set_dt<<<1, 1, 0, s>>>(d, dt);
+    // stage 0 reads sigma_n' = the time-n extension reset of the recorded state
+    adj_reset_sigma(P, f[0].phi, f[0].sxx, f[0].syy, f[0].sxy, a.s0x, a.s0y, a.s0c, s);
+    f[0].sxx = a.s0x; f[0].syy = a.s0y; f[0].sxy = a.s0c;
+    zero(h, a.acc, a.acc_words);
+    const AdjOut so{a.sU, a.sV, a.sphi, a.ssxx, a.ssyy, a.ssxy};
+    const AdjParam par{a.bub, a.but, a.bvl, a.bvr, a.G};
+    auto tend = [&](int q) {
+        return AdjTend{a.lEu[q], a.lEv[q], a.lIu[q], a.lIv[q], a.lEphi[q], a.lExx[q], a.lEyy[q], a.lExy[q]};
+    };
+    auto clear_stage = [&] {
+        zero(h, a.sU, nu); zero(h, a.sV, nv);
+        zero(h, a.sphi, N); zero(h, a.ssxx, N); zero(h, a.ssyy, N); zero(h, a.ssxy, N);
+    };
+    for (int st = 3; st >= 1; --st) {
+        if (st == 3) {  // the last stage's fields are the state after the step
+            const double* src[6] = {a.lU, a.lV, a.lphi, a.lsxx, a.lsyy, a.lsxy};
+            double* dst[6] = {a.sU, a.sV, a.sphi, a.ssxx, a.ssyy, a.ssxy};
+            const size_t n[6] = {nu, nv, N, N, N, N};
+            for (int k = 0; k < 6; ++k)
+                check_cuda(cudaMemcpyAsync(dst[k], src[k], n[k] * sizeof(double), cudaMemcpyDeviceToDevice, s),
+                           "adjoint");
+        } else {
+            clear_stage();
+            adj_tendencies(P, f[st], tend(st), so, par, a.sc, &d->st, s);
+            h->launches += 12;
+        }
+        const double* phis = st == 3 ? phi3 : f[st].phi;
+        // velocity path: projection, viscous solve, right-hand side
+        adj_projection(h, st, a.sU, a.sV, a.lpu, a.lpv);
+        const double* ru = a.lpu;
+        const double* rv = a.lpv;
+        if (h->visc) {
+            adj_viscous(h, st, phis, a.lpu, a.lpv);
+            ru = h->vs.x_u;
+            rv = h->vs.x_v;
+        }
+        adj_velocity_rhs(P, st, dt, ru, rv, a.luu, a.luv, a.lEu, a.lEv, a.lIu, a.lIv, par, s);
+        // scalar path: extension reset at phi_s, stage combination
+        adj_combine(P, st, dt, phis, a.sphi, a.ssxx, a.ssyy, a.ssxy, a.lphin, a.lsxn, a.lsyn, a.lscn, a.lEphi,
+                    a.lExx, a.lEyy, a.lExy, s);
+        h->launches += 2;
+    }
+    clear_stage();
+    adj_tendencies(P, f[0], tend(0), so, par, a.sc, &d->st, s);
+    adj_step_start(P, f[0].phi, a.sU, a.sV, a.luu, a.luv, a.sphi, a.lphin, a.ssxx, a.ssyy, a.ssxy, a.lsxn, a.lsyn,
+                   a.lscn, a.lU, a.lV, a.lphi, a.lsxx, a.lsyy, a.lsxy, s);
+    h->launches += 15;
+}
+
+void require_adjoint(const efsi_handle* h) {
+    const char* why = adjoint_unsupported(h->P, h->resource, h->growth);
+    if (why[0]) throw Err{EFSI_UNSUPPORTED, why};
 }
 
 template <class F>
@@ -1447,6 +1669,199 @@ int efsi_state_diagnostics(efsi_handle* h, const efsi_diag_config* cfg, efsi_dia
                                        (int64_t)s[4], m[5], s[3] / s[1]};
             }
         }
+    });
+}
+
+int efsi_forward_checkpointed(efsi_handle* h, double t0, const double* dts, int32_t n, int32_t every,
+                              efsi_step_report* reports) {
+    return guarded(h, [&] {
+        if (n < 1 || !dts) throw Err{EFSI_ARG, "dts must hold n >= 1 step sizes"};
+        if (h->step_block.code != EFSI_OK) throw h->step_block;
+        require_adjoint(h);
+        if (every <= 0) every = (int)std::ceil(std::sqrt((double)n));
+        every = std::max(1, std::min(std::min(every, n), kMaxBatch));
+        const int segs = (n + every - 1) / every;
+        if (segs > h->adj_ckpt_cap) {
+            if (h->ckpt) cudaFree(h->ckpt);
+            h->ckpt = nullptr;
+            h->adj_ckpt_cap = 0;
+            check_cuda(cudaMalloc(&h->ckpt, (size_t)segs * h->ckpt_stride() * sizeof(double)), "checkpoints");
+            h->adj_ckpt_cap = segs;
+        }
+        h->adj_n = 0;
+        reset_call_stats(h);
+        call_begin(h);
+        long long launches = 0;
+        int its[3][4] = {};
+        double t = t0;
+        for (int seg = 0; seg < segs; ++seg) {
+            const int k0 = seg * every, m = std::min(every, n - k0);
+            state_copy(h, h->ckpt + (size_t)seg * h->ckpt_stride(), true);
+            run_steps(h, t, dts + k0, m, reports ? reports + k0 : nullptr);
+            launches += h->stats.kernel_launches;
+            for (int b = 0; b < 4; ++b) {
+                its[0][b] += h->stats.projection_iterations[b];
+                its[1][b] += h->stats.velocity_iterations[b];
+                its[2][b] += h->stats.resource_iterations[b];
+            }
+            for (int k = 0; k < m; ++k) t += dts[k0 + k];
+        }
+        call_end(h);
+        h->adj_n = n;
+        h->adj_every = every;
+        h->adj_t0 = t0;
+        h->adj_dts.assign(dts, dts + n);
+        h->stats.kernel_launches = launches;
+        for (int b = 0; b < 4; ++b) {
+            h->stats.projection_iterations[b] = its[0][b];
+            h->stats.velocity_iterations[b] = its[1][b];
+            h->stats.resource_iterations[b] = its[2][b];
+        }
+    });
+}
+
+int efsi_backward(efsi_handle* h, const double* lam_U, const double* lam_V, const double* lam_phi,
+                  const double* lam_sxx, const double* lam_syy, const double* lam_sxy, double* grad_U,
+                  double* grad_V, double* grad_phi, double* grad_sxx, double* grad_syy, double* grad_sxy,
+                  efsi_gradient* grad) {
+    return guarded(h, [&] {
+        if (h->adj_n <= 0) throw Err{EFSI_ARG, "efsi_backward needs a preceding efsi_forward_checkpointed"};
+        require_adjoint(h);
+        ensure_adjoint_buffers(h);
+        const int n = h->adj_n, every = h->adj_every, segs = (n + every - 1) / every;
+        if (every > h->adj_tape_cap) {  // the recording graph holds the tape address: capture it again
+            if (h->tape) cudaFree(h->tape);
+            h->tape = nullptr;
+            h->adj_tape_cap = 0;
+            efsi_handle::GraphSlot& G = h->gs[1];
+            if (G.exec) { cudaGraphExecDestroy(G.exec); G.exec = nullptr; }
+            if (G.graph) { cudaGraphDestroy(G.graph); G.graph = nullptr; }
+            check_cuda(cudaMalloc(&h->tape, (size_t)every * h->tape_stride() * sizeof(double)), "tape");
+            h->adj_tape_cap = every;
+        }
+        efsi_handle::AdjBufs& a = h->ab;
+        const size_t N = h->nc, nu = h->nu, nv = h->nv;
+        const size_t nbx = (size_t)h->Nx + 1, nby = (size_t)h->Ny + 1;
+        reset_call_stats(h);
+        call_begin(h);
+        state_copy(h, a.final_state, true);
+        auto seed = [&](double* dst, const double* src, size_t m) {
+            if (src) h2d(h, dst, src, m);
+            else zero(h, dst, m);
+        };
+        seed(a.lU, lam_U, nu); seed(a.lV, lam_V, nv); seed(a.lphi, lam_phi, N);
+        seed(a.lsxx, lam_sxx, N); seed(a.lsyy, lam_syy, N); seed(a.lsxy, lam_sxy, N);
+        zero(h, a.bub, nbx); zero(h, a.but, nbx); zero(h, a.bvl, nby); zero(h, a.bvr, nby); zero(h, a.G, 1);
+        std::vector<double> tseg(segs);
+        double t = h->adj_t0;
+        for (int seg = 0; seg < segs; ++seg) {
+            tseg[seg] = t;
+            for (int k = seg * every; k < std::min(n, (seg + 1) * every); ++k) t += h->adj_dts[k];
+        }
+        struct Recording {  // recording is on only while a segment is recomputed
+            efsi_handle* h;
+            ~Recording() { h->recording = false; }
+        } guard{h};
+        for (int seg = segs - 1; seg >= 0; --seg) {
+            const int k0 = seg * every, m = std::min(every, n - k0);
+            state_copy(h, h->ckpt + (size_t)seg * h->ckpt_stride(), false);
+            h->recording = true;
+            run_steps(h, tseg[seg], h->adj_dts.data() + k0, m, nullptr);  // recompute, recording the tape
+            h->recording = false;
+            for (int j = m - 1; j >= 0; --j) reverse_step(h, j, h->adj_dts[k0 + j]);
+            fetch_dev(h);
+            raise_if_failed(h);
+        }
+        state_copy(h, a.final_state, false);
+        if (grad_U) d2h(h, grad_U, a.lU, nu);
+        if (grad_V) d2h(h, grad_V, a.lV, nv);
+        if (grad_phi) d2h(h, grad_phi, a.lphi, N);
+        if (grad_sxx) d2h(h, grad_sxx, a.lsxx, N);
+        if (grad_syy) d2h(h, grad_syy, a.lsyy, N);
+        if (grad_sxy) d2h(h, grad_sxy, a.lsxy, N);
+        if (grad) {
+            d2h(h, &grad->elastic_coefficient, a.G, 1);
+            if (grad->U_bottom) d2h(h, grad->U_bottom, a.bub, nbx);
+            if (grad->U_top) d2h(h, grad->U_top, a.but, nbx);
+            if (grad->V_left) d2h(h, grad->V_left, a.bvl, nby);
+            if (grad->V_right) d2h(h, grad->V_right, a.bvr, nby);
+        }
+        call_end(h);
+    });
+}
+
+int efsi_tendencies_adjoint(efsi_handle* h, const double* U, const double* V, const double* phi, const double* sxx,
+                            const double* syy, const double* sxy, const double* lam_Eu, const double* lam_Ev,
+                            const double* lam_Iu, const double* lam_Iv, const double* lam_Ephi,
+                            const double* lam_Exx, const double* lam_Eyy, const double* lam_Exy, double* out_U,
+                            double* out_V, double* out_phi, double* out_sxx, double* out_syy, double* out_sxy,
+                            efsi_gradient* grad) {
+    return guarded(h, [&] {
+        if (!U || !V || !phi || !sxx || !syy || !sxy) throw Err{EFSI_ARG, "stage fields must not be NULL"};
+        require_adjoint(h);
+        ensure_adjoint_buffers(h);
+        efsi_handle::AdjBufs& a = h->ab;
+        const size_t N = h->nc, nu = h->nu, nv = h->nv;
+        const size_t nbx = (size_t)h->Nx + 1, nby = (size_t)h->Ny + 1;
+        DevBlock* d = h->dev;
+        k_reset_call<<<1, 1, 0, h->stream>>>(d);
+        h2d(h, h->Us, U, nu); h2d(h, h->Vs, V, nv); h2d(h, h->phis, phi, N);
+        h2d(h, h->sxs, sxx, N); h2d(h, h->sys, syy, N); h2d(h, h->sxys, sxy, N);
+        auto seed = [&](double* dst, const double* src, size_t m) {
+            if (src) h2d(h, dst, src, m);
+            else zero(h, dst, m);
+        };
+        seed(a.lEu[0], lam_Eu, N); seed(a.lEv[0], lam_Ev, N); seed(a.lIu[0], lam_Iu, N); seed(a.lIv[0], lam_Iv, N);
+        seed(a.lEphi[0], lam_Ephi, N); seed(a.lExx[0], lam_Exx, N); seed(a.lEyy[0], lam_Eyy, N);
+        seed(a.lExy[0], lam_Exy, N);
+        zero(h, a.sU, nu); zero(h, a.sV, nv); zero(h, a.sphi, N);
+        zero(h, a.ssxx, N); zero(h, a.ssyy, N); zero(h, a.ssxy, N);
+        zero(h, a.bub, nbx); zero(h, a.but, nbx); zero(h, a.bvl, nby); zero(h, a.bvr, nby); zero(h, a.G, 1);
+        adj_tendencies(h->P, AdjIn{h->Us, h->Vs, h->phis, h->sxs, h->sys, h->sxys},
+                       AdjTend{a.lEu[0], a.lEv[0], a.lIu[0], a.lIv[0], a.lEphi[0], a.lExx[0], a.lEyy[0], a.lExy[0]},
+                       AdjOut{a.sU, a.sV, a.sphi, a.ssxx, a.ssyy, a.ssxy},
+                       AdjParam{a.bub, a.but, a.bvl, a.bvr, a.G}, a.sc, &d->st, h->stream);
+        check_cuda(cudaGetLastError(), "tendencies adjoint");
+        fetch_dev(h);
+        raise_if_failed(h);
+        if (out_U) d2h(h, out_U, a.sU, nu);
+        if (out_V) d2h(h, out_V, a.sV, nv);
+        if (out_phi) d2h(h, out_phi, a.sphi, N);
+        if (out_sxx) d2h(h, out_sxx, a.ssxx, N);
+        if (out_syy) d2h(h, out_syy, a.ssyy, N);
+        if (out_sxy) d2h(h, out_sxy, a.ssxy, N);
+        if (grad) {
+            d2h(h, &grad->elastic_coefficient, a.G, 1);
+            if (grad->U_bottom) d2h(h, grad->U_bottom, a.bub, nbx);
+            if (grad->U_top) d2h(h, grad->U_top, a.but, nbx);
+            if (grad->V_left) d2h(h, grad->V_left, a.bvl, nby);
+            if (grad->V_right) d2h(h, grad->V_right, a.bvr, nby);
+        }
+        check_cuda(cudaStreamSynchronize(h->stream), "tendencies adjoint");
+    });
+}
+
+int efsi_project_adjoint(efsi_handle* h, const double* lam_U, const double* lam_V, double* lam_U_in,
+                         double* lam_V_in) {
+    return guarded(h, [&] {
+        if (!lam_U || !lam_V || !lam_U_in || !lam_V_in) throw Err{EFSI_ARG, "arrays must not be NULL"};
+        ensure_adjoint_buffers(h);
+        efsi_handle::AdjBufs& a = h->ab;
+        DevBlock* d = h->dev;
+        reset_call_stats(h);
+        k_reset_call<<<1, 1, 0, h->stream>>>(d);
+        h2d(h, a.sU, lam_U, h->nu);
+        h2d(h, a.sV, lam_V, h->nv);
+        adj_proj_rhs(h->P, h->pj, a.sU, a.sV, &d->ps, h->slot[0], h->stream);
+        proj_solve(h, 0, kAdjointReltol, a.zq);
+        proj_mean(h->P, h->pj, &d->ps, h->slot[6], h->stream);
+        adj_proj_finish_full(h->P, h->pj, a.sU, a.sV, &d->ps, a.lU, a.lV, h->stream);
+        fetch_dev(h);
+        raise_if_failed(h);
+        d2h(h, lam_U_in, a.lU, h->nu);
+        d2h(h, lam_V_in, a.lV, h->nv);
+        check_cuda(cudaStreamSynchronize(h->stream), "project adjoint");
+        h->stats.projection_iterations[0] = h->host->iters[KIND_PROJ][0];
     });
 }
 

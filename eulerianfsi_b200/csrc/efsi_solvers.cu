@@ -1818,6 +1818,12 @@ __global__ void k_proj_correct(Params P, MGLevel L, const double* __restrict__ x
     }
 }
 
+void proj_mean(const Params& P, const Projection& pj, ProjScal* ps, const RedSlot& rs, cudaStream_t s) {
+    const MGLevel& L = pj.lev[0];
+    k_proj_mean<<<persistent_grid(tiles2(L.nx, L.ny), P.nsm, 8), dim3(BX, BY), 0, s>>>(L, pj.x, ps, rs,
+                                                                                     pj.nullspace ? 1 : 0);
+}
+
 void proj_finish(const Params& P, const Projection& pj, const double* G, double* q_out, double* U_out, double* V_out,
                  ProjScal* ps, double* stage_linf, const RedSlot& rs1, const RedSlot& rs2, DevStatus* st,
                  cudaStream_t s) {

@@ -146,6 +146,8 @@ void proj_update_vcycle(const Params& P, const Projection& pj, int parity, CGSca
 void proj_finish(const Params& P, const Projection& pj, const double* G, double* q_out, double* U_out,
                  double* V_out, ProjScal* ps, double* stage_linf, const RedSlot& rs1, const RedSlot& rs2,
                  DevStatus* st, cudaStream_t s);
+// ps->v[6] = mean of the solution pj.x with a constant nullspace (0 otherwise).
+void proj_mean(const Params& P, const Projection& pj, ProjScal* ps, const RedSlot& rs, cudaStream_t s);
 // Kernel launches of proj_update_vcycle and of proj_cg_init (statistics).
 int proj_update_vcycle_kernels(const Projection& pj);
 int proj_init_kernels(const Projection& pj);

@@ -53,6 +53,73 @@ def objective(state: FSIState, workload, shear_modulus: float) -> float:
     return y_centroid + ENERGY_WEIGHT * float(np.sum(phi * density * area))
 
 
+def objective_cotangent(state: FSIState, workload, shear_modulus: float):
+    """(J, dJ/d(final state) as a dict of cell arrays, dJ/dG at fixed state) of the
+    objective above: the centroid term differentiates to dA (y - y_c) / M, the energy
+    term to w (G/2)(tr - 2 - log det) dA in phi and w phi (G/2)(1 - s_yy/det,
+    1 - s_xx/det, 2 s_xy/det) dA in the tensor components."""
+    area = np.outer(workload.metrics.dx_c, workload.metrics.dy_c)
+    phi, sxx, syy, sxy = state.phi, state.sigma_xx, state.sigma_yy, state.sigma_xy
+    mass = float(np.sum(phi * area))
+    if not mass > np.finfo(np.float64).eps:
+        raise ArgumentError("Phase integral is too small to define a centroid.")
+    y_p = np.asarray(workload.grid.y_p)[None, :]
+    y_centroid = float(np.sum(phi * area * y_p)) / mass
+    det = sxx * syy - sxy ** 2
+    if not np.all(det > 0.0):
+        raise DomainError("structure tensor is not SPD; its elastic energy is undefined")
+    half_g = 0.5 * shear_modulus
+    density = half_g * (sxx + syy - 2.0 - np.log(det))
+    energy = float(np.sum(phi * density * area))
+    J = y_centroid + ENERGY_WEIGHT * energy
+    w = ENERGY_WEIGHT * area
+    cot = {"phi": np.asfortranarray(area * (y_p - y_centroid) / mass + w * density),
+           "sigma_xx": np.asfortranarray(w * phi * half_g * (1.0 - syy / det)),
+           "sigma_yy": np.asfortranarray(w * phi * half_g * (1.0 - sxx / det)),
+           "sigma_xy": np.asfortranarray(w * phi * half_g * (2.0 * sxy / det))}
+    dJ_dG = ENERGY_WEIGHT * energy / shear_modulus if shear_modulus != 0.0 else 0.0
+    return J, cot, dJ_dG
+
+
+def circle_center_derivative(grid, center, radius, epsilon):
+    """d(phi_0)/d(center x) and /d(center y) of initialize_circle's tanh profile
+    phi_0 = (1 - tanh((|x - c| - r) / eps)) / 2."""
+    X = np.asarray(grid.x_p)[:, None] * np.ones((1, grid.Ny))
+    Y = np.ones((grid.Nx, 1)) * np.asarray(grid.y_p)[None, :]
+    dx, dy = X - center[0], Y - center[1]
+    rho = np.hypot(dx, dy)
+    t = np.tanh((rho - radius) / epsilon)
+    g = np.where(rho > 0.0, 0.5 * (1.0 - t * t) / (epsilon * np.where(rho > 0.0, rho, 1.0)), 0.0)
+    return g * dx, g * dy
+
+
+def adjoint_gradient(N: int = 256, T: float = 2.0, p=DEFAULT_PARAMETERS, reltol: float = FD_RELTOL,
+                     every: int = 0, timings: dict | None = None) -> dict:
+    """J and dJ/dp for p = (G, lid speed, centre x, y) from one checkpointed forward run
+    and one reverse sweep of the discrete adjoint.  `timings` receives the device
+    milliseconds of the forward run and of the reverse sweep (which includes its
+    recomputation of every checkpoint segment)."""
+    from . import adjoint
+    G, lid, cx, cy = (float(v) for v in p)
+    w = workloads.cavity_disk_sensitivity(N, tuple(p), T, projection_reltol=reltol, velocity_reltol=reltol)
+    ctx = build_imex_context(w.metrics, w.bcs, w.models, numerics=w.numerics)
+    state = w.state.copy()
+    adjoint.forward_checkpointed(state, 0.0, np.full(w.steps, w.dt), ctx, every)
+    forward_ms = ctx.handle.stats()["device_ms"]
+    J, cot, dJdG_direct = objective_cotangent(state, w, G)
+    grad_state, pg = adjoint.backward(ctx, cot)
+    backward_ms = ctx.handle.stats()["device_ms"]
+    ctx.handle.close()
+    h = 1.0 / N
+    dcx, dcy = circle_center_derivative(w.grid, (cx, cy), 0.2, 1.5 * h)
+    # the lid speed is the (uniform) U-top wall datum: every entry moves with it
+    gradient = [pg.elastic_coefficient + dJdG_direct, float(np.sum(pg.U_top)),
+                float(np.sum(grad_state.phi * dcx)), float(np.sum(grad_state.phi * dcy))]
+    if timings is not None:
+        timings.update(forward_ms=forward_ms, backward_ms=backward_ms)
+    return {"J": J, "gradient": gradient, "steps": w.steps, "forward_ms": forward_ms, "backward_ms": backward_ms}
+
+
 def cuda_final_state(w, timings: list | None = None) -> FSIState:
     """Run workload `w` for w.steps device-resident steps on the CUDA library and
     return the final state; the run's device milliseconds are appended to

@@ -384,6 +384,55 @@ EFSI_API int efsi_state_diagnostics(efsi_handle* h, const efsi_diag_config* conf
  * efsi_stats.  Tracing aid of the benchmark; no reference counterpart. */
 EFSI_API int efsi_set_timed_site(efsi_handle* h, int32_t site);
 
+/* ---- differentiation form ------------------------------------------------------
+ * A discrete adjoint of integrate_step! (TimeIntegrationIMEX.jl:1152-1256) for the
+ * ChainRulesCore.rrule of a run of steps; the reference has no adjoint, so these
+ * entry points have no counterpart there.  The adjoint differentiates the ACDI
+ * phase field (fixed mobility), constant or no viscosity, linear elastic stress,
+ * Maxwell relaxation, every structure extension and body force, on every boundary
+ * kind the step accepts; growth, resource transport and capillarity return
+ * EFSI_UNSUPPORTED.  Parameters: the elastic coefficient G and the tangential wall
+ * velocity data (a moving lid is U top).  Explicit stencils are transposed exactly
+ * (upwind and clamp switches are held at the forward branch); the projection and
+ * viscous solves are transposed as exact inverses, solved to a relative residual of
+ * 1e-13. */
+typedef struct efsi_gradient {
+    double  elastic_coefficient;  /* dJ/dG of LinearInternalTensorStress(G)                */
+    double *U_bottom, *U_top;     /* dJ/d(U wall data), Nx+1 entries each; may be NULL      */
+    double *V_left, *V_right;     /* dJ/d(V wall data), Ny+1 entries each; may be NULL      */
+} efsi_gradient;
+
+/* efsi_step_n that also keeps the state (and the projection warm start) every `every`
+ * steps in device memory (every <= 0: ceil(sqrt(n)), at most 1024), for a following
+ * efsi_backward.  The device state advances exactly as with efsi_step_n. */
+EFSI_API int efsi_forward_checkpointed(efsi_handle* h, double t0, const double* dts, int32_t n, int32_t every,
+                                       efsi_step_report* reports);
+/* Reverse sweep over the steps of the last efsi_forward_checkpointed call: given
+ * lam = dJ/d(final state) (host arrays; NULL = zero), returns dJ/d(initial state) in
+ * grad_* (NULL = not wanted) and the parameter derivatives in *grad (may be NULL).
+ * Each segment between checkpoints is recomputed forward once with its stage fields
+ * recorded, then swept backwards; the device state is left at the final state. */
+EFSI_API int efsi_backward(efsi_handle* h, const double* lam_U, const double* lam_V, const double* lam_phi,
+                           const double* lam_sxx, const double* lam_syy, const double* lam_sxy, double* grad_U,
+                           double* grad_V, double* grad_phi, double* grad_sxx, double* grad_syy,
+                           double* grad_sxy, efsi_gradient* grad);
+/* Transposed Jacobian of one stage's explicit tendencies (TimeIntegrationIMEX.jl:944-1071)
+ * at the stage fields (U, V full MAC; cell fields): given the adjoints of E_uv and I_uv
+ * (compact rows U(0:Nx-1,:), V(:,0:Ny-1), N each), of E_phi and of E_sigma (NULL = zero),
+ * writes the adjoints of the six stage fields and of the parameters.  Exposed for
+ * dot-product tests of the transposed stencils. */
+EFSI_API int efsi_tendencies_adjoint(efsi_handle* h, const double* U, const double* V, const double* phi,
+                                     const double* sxx, const double* syy, const double* sxy,
+                                     const double* lam_Eu, const double* lam_Ev, const double* lam_Iu,
+                                     const double* lam_Iv, const double* lam_Ephi, const double* lam_Exx,
+                                     const double* lam_Eyy, const double* lam_Exy, double* out_U, double* out_V,
+                                     double* out_phi, double* out_sxx, double* out_syy, double* out_sxy,
+                                     efsi_gradient* grad);
+/* Transposed efsi_project (Projection.jl:170-307) with respect to its input velocity:
+ * lam of the input faces from lam of the projected faces (full MAC arrays). */
+EFSI_API int efsi_project_adjoint(efsi_handle* h, const double* lam_U, const double* lam_V, double* lam_U_in,
+                                  double* lam_V_in);
+
 /* How efsi_integrate_step / efsi_integrate_step_host / efsi_step_n run a step:
  *   EFSI_STEP_GRAPH  (default) the whole step is one captured CUDA graph whose
  *                    solver loops are device-terminated conditional nodes;

@@ -18,7 +18,7 @@ STRUCTS = {
     "efsi_models": _abi.Models, "efsi_numerics": _abi.Numerics, "efsi_config": _abi.Config,
     "efsi_step_report": _abi.StepReportC, "efsi_projection_result": _abi.ProjectionResultC,
     "efsi_stats": _abi.Stats, "efsi_diag_config": _abi.DiagConfig, "efsi_tensor_region": _abi.TensorRegion,
-    "efsi_diagnostics": _abi.Diagnostics,
+    "efsi_diagnostics": _abi.Diagnostics, "efsi_gradient": _abi.GradientC,
 }
 
 

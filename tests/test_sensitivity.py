@@ -105,3 +105,42 @@ def test_replica_ensemble_on_two_gloo_ranks_matches_serial():
         mp.start_processes(_rank, args=(world, _free_port(), out), nprocs=world, start_method="spawn")
         for r in range(world):
             assert out[r][0] == J and out[r][1] == D.tolist()
+
+
+def test_objective_cotangent_matches_differences_of_the_objective():
+    """The host half of the adjoint gradient: dJ/d(final state) and dJ/dG of the
+    objective against central differences of sensitivity.objective."""
+    w = workloads.cavity_disk_sensitivity(N=8, T=0.025)
+    rng = np.random.default_rng(4)
+    st = w.state.copy()
+    st.phi[...] = 0.2 + 0.6 * rng.random(st.phi.shape)
+    st.sigma_xx[...] = 1.0 + 0.3 * rng.random(st.phi.shape)
+    st.sigma_yy[...] = 1.0 + 0.3 * rng.random(st.phi.shape)
+    st.sigma_xy[...] = 0.1 * rng.standard_normal(st.phi.shape)
+    G = 0.1
+    J, cot, dJdG = sens.objective_cotangent(st, w, G)
+    assert abs(J - sens.objective(st, w, G)) <= 1e-15
+    eps = 1e-6
+    for name in ("phi", "sigma_xx", "sigma_yy", "sigma_xy"):
+        d = rng.standard_normal(st.phi.shape)
+        a, b = st.copy(), st.copy()
+        getattr(a, name)[...] += eps * d
+        getattr(b, name)[...] -= eps * d
+        fd = (sens.objective(a, w, G) - sens.objective(b, w, G)) / (2 * eps)
+        assert abs(fd - float(np.sum(cot[name] * d))) <= 1e-8 * max(abs(fd), 1.0), name
+    fdG = (sens.objective(st, w, G + eps) - sens.objective(st, w, G - eps)) / (2 * eps)
+    assert abs(fdG - dJdG) <= 1e-9
+
+
+def test_circle_center_derivative_matches_differences():
+    from eulerianfsi_b200.init import initialize_circle
+    w = workloads.cavity_disk_sensitivity(N=16, T=0.025)
+    h = 1.0 / 16
+    c = (0.6, 0.5)
+    dcx, dcy = sens.circle_center_derivative(w.grid, c, 0.2, 1.5 * h)
+    eps = 1e-7
+    fx = (initialize_circle(w.grid, (c[0] + eps, c[1]), 0.2, 1.5 * h) -
+          initialize_circle(w.grid, (c[0] - eps, c[1]), 0.2, 1.5 * h)) / (2 * eps)
+    fy = (initialize_circle(w.grid, (c[0], c[1] + eps), 0.2, 1.5 * h) -
+          initialize_circle(w.grid, (c[0], c[1] - eps), 0.2, 1.5 * h)) / (2 * eps)
+    assert np.max(np.abs(fx - dcx)) <= 1e-6 and np.max(np.abs(fy - dcy)) <= 1e-6
