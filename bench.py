@@ -501,6 +501,43 @@ def run_sensitivity(args, rank, world, dist):
     print(json.dumps(res), flush=True)
 
 
+def run_adjoint(args):
+    """Differentiation form on the cavity-disk objective (N=256 to T=2 by default): the
+    gradient over (G, lid speed, disk centre x, y) from one checkpointed forward run and
+    one reverse sweep, its cost in plain forward runs, and (unless --no-fd) its agreement
+    with the central-difference gradient of the same forward (11 runs).  One JSON line."""
+    import numpy as np
+    import torch
+
+    from eulerianfsi_b200 import sensitivity as sens
+    torch.cuda.set_device(0)
+    p = sens.DEFAULT_PARAMETERS
+    plain = []
+    ev = sens.make_evaluator(args.sens_N, args.sens_T, timings=plain)
+    J_plain = ev(p)  # one plain forward run (device-resident steps, no checkpoints)
+    res = sens.adjoint_gradient(args.sens_N, args.sens_T, p, every=args.adj_every)
+    forward_ms = plain[0]
+    line = {"metric": "adjoint/forward cost", "value": (res["forward_ms"] + res["backward_ms"]) / forward_ms,
+            "unit": "forward runs per gradient", "higher_is_better": False,
+            "config": {"workload": "cavity_disk_sensitivity", "Nx": args.sens_N, "Ny": args.sens_N,
+                       "T": args.sens_T, "steps": res["steps"], "dt": 0.2 / args.sens_N, "precision": "fp64",
+                       "solver_reltol": sens.FD_RELTOL, "parameters": list(sens.PARAMETERS), "at": list(p),
+                       "checkpoint_every": args.adj_every or int(np.ceil(np.sqrt(res["steps"])))},
+            "J": res["J"], "J_plain_forward": J_plain, "gradient": res["gradient"],
+            "plain_forward_ms": forward_ms, "checkpointed_forward_ms": res["forward_ms"],
+            "backward_ms": res["backward_ms"], "dtype": "f64", "data": "synthetic"}
+    if not args.no_fd:
+        fd = sens.gradient_check(ev, p, seed=args.sens_seed)
+        g, a = np.array(fd["gradient"]), np.array(res["gradient"])
+        d = np.array(fd["direction"])
+        line["finite_differences"] = {
+            "gradient": fd["gradient"], "rel_l2_adjoint_vs_fd": float(np.linalg.norm(a - g) / np.linalg.norm(g)),
+            "directional_fd": fd["directional"], "directional_adjoint": float(a @ d),
+            "rel_diff_directional": abs(float(a @ d) - fd["directional"]) / abs(fd["directional"]),
+            "runs": fd["runs"], "rel_h": 1e-6}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -533,9 +570,16 @@ def main():
     p.add_argument("--sens-N", type=int, default=256)
     p.add_argument("--sens-T", type=float, default=2.0)
     p.add_argument("--sens-seed", type=int, default=0)
+    p.add_argument("--adjoint", action="store_true",
+                   help="discrete-adjoint gradient of the cavity-disk objective and its cost in forward runs")
+    p.add_argument("--adj-every", type=int, default=0, help="checkpoint spacing (0: ceil(sqrt(steps)))")
+    p.add_argument("--no-fd", action="store_true", help="skip the finite-difference comparison of --adjoint")
     args = p.parse_args()
     if args.configs:
         run_configs(args)
+        return
+    if args.adjoint:
+        run_adjoint(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -565,8 +565,12 @@ __device__ __forceinline__ double acdi_psi(const efsi_models& md, double p) {
     const double q = clamp01(p), e = md.pf_param[2];
     return md.pf_param[1] * log((q + e) / (1.0 - q + e));
 }
+// d(psi)/d(phi).  psi saturates on the plateaus phi <= 0 and phi >= 1 (the clamp), where
+// the slope eps / psi_floor of the open interval (1e98 eps for the default floor) is
+// not a derivative of the clamped map: the plateaus, which hold exactly 0 and 1 in the
+// disk interior and far field, take the clamp's zero slope.
 __device__ __forceinline__ double acdi_dpsi(const efsi_models& md, double p) {
-    if (p < 0.0 || p > 1.0) return 0.0;
+    if (!(p > 0.0 && p < 1.0)) return 0.0;
     const double e = md.pf_param[2];
     return md.pf_param[1] * (1.0 / (p + e) + 1.0 / (1.0 - p + e));
 }

@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import shutil
 import subprocess
 
 import numpy as np
@@ -36,8 +37,11 @@ _LIB = None
 
 
 def build(force: bool = False) -> str:
-    """Compile the oracle with its Makefile (g++ only)."""
-    if force or not os.path.exists(LIB_PATH):
+    """Compile the oracle with its Makefile (g++ only); make rebuilds it when a source
+    or the ABI header is newer than the library."""
+    if force and os.path.exists(LIB_PATH):
+        os.remove(LIB_PATH)
+    if force or not os.path.exists(LIB_PATH) or shutil.which("make"):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB_PATH
 
