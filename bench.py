@@ -527,14 +527,18 @@ def run_adjoint(args):
             "plain_forward_ms": forward_ms, "checkpointed_forward_ms": res["forward_ms"],
             "backward_ms": res["backward_ms"], "dtype": "f64", "data": "synthetic"}
     if not args.no_fd:
-        fd = sens.gradient_check(ev, p, seed=args.sens_seed)
-        g, a = np.array(fd["gradient"]), np.array(res["gradient"])
-        d = np.array(fd["direction"])
-        line["finite_differences"] = {
-            "gradient": fd["gradient"], "rel_l2_adjoint_vs_fd": float(np.linalg.norm(a - g) / np.linalg.norm(g)),
-            "directional_fd": fd["directional"], "directional_adjoint": float(a @ d),
-            "rel_diff_directional": abs(float(a @ d) - fd["directional"]) / abs(fd["directional"]),
-            "runs": fd["runs"], "rel_h": 1e-6}
+        fds = []
+        for rel_h in args.fd_rel_h:
+            fd = sens.gradient_check(ev, p, seed=args.sens_seed, rel_h=rel_h)
+            g, a = np.array(fd["gradient"]), np.array(res["gradient"])
+            d = np.array(fd["direction"])
+            fds.append({
+                "rel_h": rel_h, "gradient": fd["gradient"],
+                "rel_l2_adjoint_vs_fd": float(np.linalg.norm(a - g) / np.linalg.norm(g)),
+                "directional_fd": fd["directional"], "directional_adjoint": float(a @ d),
+                "rel_diff_directional": abs(float(a @ d) - fd["directional"]) / abs(fd["directional"]),
+                "fd_self_consistency": fd["rel_diff"], "runs": fd["runs"]})
+        line["finite_differences"] = fds
     print(json.dumps(line), flush=True)
 
 
@@ -574,6 +578,8 @@ def main():
                    help="discrete-adjoint gradient of the cavity-disk objective and its cost in forward runs")
     p.add_argument("--adj-every", type=int, default=0, help="checkpoint spacing (0: ceil(sqrt(steps)))")
     p.add_argument("--no-fd", action="store_true", help="skip the finite-difference comparison of --adjoint")
+    p.add_argument("--fd-rel-h", type=float, nargs="+", default=[1e-6],
+                   help="relative steps of the finite differences --adjoint compares against")
     args = p.parse_args()
     if args.configs:
         run_configs(args)

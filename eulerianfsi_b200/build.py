@@ -66,12 +66,29 @@ def build(force: bool = False, verbose: bool = False) -> str:
     build_dir = os.path.join(HERE, "_build")
     os.makedirs(build_dir, exist_ok=True)
 
+    def object_hash(src: str) -> str:  # the source, every header and the flags
+        h = hashlib.sha256()
+        h.update(" ".join(GENCODE + FLAGS).encode())
+        for path in [os.path.join(CSRC, src)] + _inputs()[len(SOURCES):]:
+            with open(path, "rb") as f:
+                h.update(f.read())
+        return h.hexdigest()
+
     def compile_one(src: str) -> str:
         obj = os.path.join(build_dir, src.replace(".cu", ".o"))
+        digest_o = object_hash(src)
+        try:  # an object built from the same inputs is reused
+            with open(obj + ".stamp") as f:
+                if not force and f.read().strip() == digest_o and os.path.exists(obj):
+                    return obj
+        except OSError:
+            pass
         cmd = [nvcc(), *GENCODE, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
+        with open(obj + ".stamp", "w") as f:
+            f.write(digest_o + "\n")
         return obj
 
     with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as pool:

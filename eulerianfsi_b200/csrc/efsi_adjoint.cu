@@ -158,15 +158,6 @@ __device__ __forceinline__ Dn<K> dlog(const Dn<K>& a) {
     return r;
 }
 template <int K>
-__device__ __forceinline__ Dn<K> dtanh(const Dn<K>& a) {
-    Dn<K> r;
-    r.v = tanh(a.v);
-    const double g = 1.0 - r.v * r.v;
-#pragma unroll
-    for (int k = 0; k < K; ++k) r.d[k] = g * a.d[k];
-    return r;
-}
-template <int K>
 __device__ __forceinline__ Dn<K> dpow(const Dn<K>& a, double p) {
     Dn<K> r;
     r.v = pow(a.v, p);
@@ -182,6 +173,21 @@ __device__ __forceinline__ Dn<K> dhypot(const Dn<K>& a, const Dn<K>& b) {
     const double ia = r.v > 0.0 ? a.v / r.v : 0.0, ib = r.v > 0.0 ? b.v / r.v : 0.0;
 #pragma unroll
     for (int k = 0; k < K; ++k) r.d[k] = ia * a.d[k] + ib * b.d[k];
+    return r;
+}
+// sech^2(x) = 1 - tanh^2(x) from e = exp(-2|x|): 4e / (1 + e)^2 keeps its full relative
+// accuracy where it is tiny (|x| large), unlike the difference 1 - tanh^2, whose rounding
+// error there is larger than the value itself.
+template <int K>
+__device__ __forceinline__ Dn<K> dsech2(const Dn<K>& a) {
+    Dn<K> r;
+    const double e = exp(-2.0 * fabs(a.v));
+    const double den = 1.0 + e;
+    r.v = 4.0 * e / (den * den);
+    const double th = (a.v >= 0.0 ? 1.0 : -1.0) * (1.0 - e) / den;  // tanh(x)
+    const double g = -2.0 * th * r.v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = g * a.d[k];
     return r;
 }
 // clamp to [0, 1]: slope 1 inside, 0 outside
@@ -565,13 +571,22 @@ __device__ __forceinline__ double acdi_psi(const efsi_models& md, double p) {
     const double q = clamp01(p), e = md.pf_param[2];
     return md.pf_param[1] * log((q + e) / (1.0 - q + e));
 }
-// d(psi)/d(phi).  psi saturates on the plateaus phi <= 0 and phi >= 1 (the clamp), where
-// the slope eps / psi_floor of the open interval (1e98 eps for the default floor) is
-// not a derivative of the clamped map: the plateaus, which hold exactly 0 and 1 in the
-// disk interior and far field, take the clamp's zero slope.
+#ifndef EFSI_ADJ_NORMAL_FLOOR
+#define EFSI_ADJ_NORMAL_FLOOR 1e-6
+#endif
+#ifndef EFSI_ADJ_PSI_SLOPE_FLOOR
+#define EFSI_ADJ_PSI_SLOPE_FLOOR 1e-8
+#endif
+// d(psi)/d(phi) as the reverse sweep uses it.  psi saturates on the plateaus phi <= 0 and
+// phi >= 1 (the clamp), which take the clamp's zero slope.  Inside (0, 1) the slope
+// eps (1/(q + e) + 1/(1 - q + e)) reaches eps / min(q, 1 - q) next to the plateaus: cells
+// of the disk interior at phi = 1 - 1e-16 give 1e13 eps, where the forward map, whose phi
+// resolves 1 - phi to a few bits, responds to no admissible perturbation, while the
+// reverse sweep multiplies every adjoint through it (1e30 per step at 256^2 measured).
+// The slope is therefore taken with the floor max(e, EFSI_ADJ_PSI_SLOPE_FLOOR).
 __device__ __forceinline__ double acdi_dpsi(const efsi_models& md, double p) {
     if (!(p > 0.0 && p < 1.0)) return 0.0;
-    const double e = md.pf_param[2];
+    const double e = fmax(md.pf_param[2], EFSI_ADJ_PSI_SLOPE_FLOOR);
     return md.pf_param[1] * (1.0 / (p + e) + 1.0 / (1.0 - p + e));
 }
 
@@ -600,10 +615,23 @@ __device__ void acdi_normal_d(const Params& P, const double* psi, int ci, int cj
     Dn<5> gt = nb[4] >= 0 ? (at(4) - c) * P.g.ihy : wall(TOP, true, P.g.hy);
     Dn<5> gx = 0.5 * gl + 0.5 * gr;
     Dn<5> gy = 0.5 * gb + 0.5 * gt;
+    // value: g / sqrt(|g|^2 + delta^2) as the forward has it.  Derivative: the same map
+    // with the gradient floor max(delta, EFSI_ADJ_NORMAL_FLOOR); where psi is flat (the
+    // saturated disk interior, whose rounded phi makes neighbouring psi equal) the
+    // forward's 1/delta = 1e14 sensitivity meets flux amplitudes of 1e-16 and would close
+    // a loop in the reverse sweep that grows without bound.
     const double delta = P.md.pf_param[3];
-    Dn<5> mag = dsqrt(gx * gx + gy * gy + delta * delta);
-    nx = gx / mag;
-    ny = gy / mag;
+    const double da = fmax(delta, EFSI_ADJ_NORMAL_FLOOR);
+    const double g2 = gx.v * gx.v + gy.v * gy.v;
+    const double m = sqrt(g2 + delta * delta), ma = sqrt(g2 + da * da);
+    nx.v = gx.v / m;
+    ny.v = gy.v / m;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const double dm = (gx.v * gx.d[k] + gy.v * gy.d[k]) / ma;
+        nx.d[k] = (gx.d[k] - gx.v / ma * dm) / ma;
+        ny.d[k] = (gy.d[k] - gy.v / ma * dm) / ma;
+    }
 }
 
 // psi and the cell normals of the stage field; clears the layer adjoints.
@@ -640,8 +668,10 @@ __device__ void acdi_face_rev(const Params& P, const double* phi, const AdjScrat
     Dn<7> pf = 0.5 * pL + 0.5 * pR;
     Dn<7> cflux = u * pf;
     Dn<7> psf = 0.5 * sL + 0.5 * sR;
-    Dn<7> th = dtanh(psf / (2.0 * eps));
-    Dn<7> amp = 0.25 * (1.0 - th * th);
+    // amp = (1 - tanh^2(psf / 2 eps)) / 4 as the forward flux has it, evaluated without
+    // cancellation: in the saturated layers amp ~ min(phi, 1 - phi) multiplies a psi
+    // slope ~ eps / min(phi, 1 - phi), and only accurate factors give their O(1) product
+    Dn<7> amp = 0.25 * dsech2(psf / (2.0 * eps));
     Dn<7> nf = 0.5 * nL + 0.5 * nR;
     Dn<7> rflux = geff * (eps * ((pR - pL) * h_i) - amp * nf);
     Dn<7> F = lc * cflux + lr * rflux;
