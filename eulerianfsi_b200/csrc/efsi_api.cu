@@ -816,7 +816,24 @@ void enqueue_step(efsi_handle* h) {
                 DtCoef alpha{dtp, c_AI_diag[st]};
                 const SolveOpts o = solve_opts(P.nu, P.nu.velocity_method);
                 const int maxit = solve_limit(o);
-                if (h->mixed) {
+                if (h->mixed && visc_cheb_applies(P)) {
+                    solve(
+                        h, KIND_VISC, st, &d->cg_visc, maxit, 2, 2,
+                        [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
+                            site(h, EFSI_SITE_VISC_INIT, 8.0 * N * 10.0, [&] {
+                                visc_cheb_init(P, alpha, o, h->U, h->V, h->rhs_u, h->rhs_v, h->vs, h->vm,
+                                               &d->cg_visc, h->slot[0], io, ch, ss);
+                            });
+                            h->launches += 2;
+                        },
+                        [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {
+                            for (int k = 0; k < 2; ++k)  // FP32 e, r, d in and out: 48 B per point per launch
+                                site(h, EFSI_SITE_VISC_CG, 4.0 * N * 12.0, [&] {
+                                    visc_cheb_iter(P, alpha, h->rhs_u, h->rhs_v, h->vs, h->vm, k, &d->cg_visc,
+                                                   h->slot[2], io, ch, ss);
+                                });
+                        });
+                } else if (h->mixed) {
                     solve(
                         h, KIND_VISC, st, &d->cg_visc, maxit, 2, 2,
                         [&](cudaStream_t ss, int* io, cudaGraphConditionalHandle ch) {

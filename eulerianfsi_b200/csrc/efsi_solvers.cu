@@ -708,6 +708,311 @@ void visc_mx_iter(const Params& P, DtCoef alpha, const double* phi, const double
         P, alpha, SolveOpts{}, phi, visc_mx_args(w, m, rhs_u, rhs_v, parity), cg, rs, iters_out, cond);
 }
 
+// ---- precision form with a constant viscosity: FP32 Chebyshev inner solver -----------
+// Phases of the body launches: ITER (kChebSteps FP32 Chebyshev steps on the correction
+// equation), APPLY (x += e in FP64), REFINE (r = rhs - (I - alpha A) x in FP64; stop or
+// start the next inner cycle from it).  Chebyshev recurrence for M e = r with
+// spec(M) in [1, 1 + 2 delta] (Saad, Iterative Methods for Sparse Linear Systems,
+// Algorithm 12.1): theta = 1 + delta, sigma = theta / delta, rho_0 = 1 / sigma,
+// d_0 = r_0 / theta; per step e += d, r -= M d, rho' = 1 / (2 sigma - rho),
+// d = rho' rho d + (2 rho' / delta) r.
+enum { CH_ITER = 0, CH_APPLY = 1, CH_REFINE = 2 };
+constexpr int CK = kChebSteps, CTX = 32, CTY = 16, CWX = CTX + 2 * CK, CWY = CTY + 2 * CK;
+// Residual drop one FP32 inner cycle aims for (FP32 resolves about 1e-7).
+constexpr double kChebDrop = 1e-5;
+
+struct ChebArgs {
+    const float *r_u, *r_v, *d_u, *d_v, *e_u, *e_v;  // set read by this launch
+    float *rn_u, *rn_v, *dn_u, *dn_v, *en_u, *en_v;  // set written by this launch
+    double *x_u, *x_v;
+    const double *rhs_u, *rhs_v;
+};
+
+// theta and delta of the free block of I - alpha A for a constant viscosity mu:
+// spec in [1, 1 + alpha g] with g = mu (max(8/hx^2 + 4/hy^2, 4/hx^2 + 8/hy^2) +
+// 4/(hx hy)), the Gershgorin bound of the rows of -A (wall rows sum to less).
+__device__ __forceinline__ void cheb_bounds(const Params& P, double alpha, double& theta, double& delta) {
+    const double ix2 = P.g.ihx * P.g.ihx, iy2 = P.g.ihy * P.g.ihy;
+    const double g = P.md.viscosity_fluid * (fmax(8.0 * ix2 + 4.0 * iy2, 4.0 * ix2 + 8.0 * iy2) + 4.0 * P.g.ihx * P.g.ihy);
+    delta = 0.5 * alpha * g;
+    theta = 1.0 + delta;
+}
+// Chebyshev steps of one inner cycle for the residual drop `drop` (|r_n| <= |r_0| /
+// T_n(sigma)), rounded up to whole launches.
+__device__ __forceinline__ int cheb_steps(double theta, double delta, double drop) {
+    if (!(delta > 1e-300)) return CK;
+    const double n = acosh(1.0 / drop) / acosh(theta / delta);
+    const int k = max(1, (int)ceil(n));
+    return ((k + CK - 1) / CK) * CK;
+}
+
+// Shared-memory view (doubles converted from the FP32 region) for the general stencil
+// at cells next to an edge; requests use global indices, wrapped ones map back.
+struct ChebTile {
+    const float* su;
+    const float* sv;
+    int i0, j0, Nx, Ny;
+    __device__ __forceinline__ int slot(int c, int r) const {
+        int lc = c - i0 + CK, lr = r - j0 + CK;
+        if (lc < 0) lc += Nx; else if (lc >= CWX) lc -= Nx;
+        if (lr < 0) lr += Ny; else if (lr >= CWY) lr -= Ny;
+        return lr * CWX + lc;
+    }
+    __device__ __forceinline__ double U(int c, int r) const { return su[slot(c, r)]; }
+    __device__ __forceinline__ double V(int c, int r) const { return sv[slot(c, r)]; }
+};
+
+// REFINE (and the START of a solve): stage x (APPLY has added the last correction) over
+// a 32x8 tile and one-cell ring, r = rhs - (x - alpha A x) in FP64 at the tile, |r|^2 and
+// |b|^2; the next inner cycle starts from r: r_set = r, d_set = r / theta, e_set = 0.
+template <bool START>
+__device__ void cheb_refine(const Params& P, double alpha, double theta, const ChebArgs& v, double* sm, double (&acc)[2]) {
+    double* su = sm;
+    double* sv = sm + VSX * VSY;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + ty * VTX;
+    const int Nx = P.g.Nx, Ny = P.g.Ny;
+    const int ntx = (Nx + VTX - 1) / VTX, nt = ntx * ((Ny + VTY - 1) / VTY);
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int i0 = (t % ntx) * VTX, j0 = (t / ntx) * VTY;
+        const int i = i0 + tx, j = j0 + ty;
+        for (int q = tid; q < VSX * VSY; q += VTX * VTY) {
+            const int gi = i0 + q % VSX - 1, gj = j0 + q / VSX - 1;
+            const bool inx = gi >= 0 && gi < Nx, iny = gj >= 0 && gj < Ny;
+            double hu = 0.0, hv = 0.0;
+            if ((inx || P.g.px) && (iny || P.g.py)) {
+                const size_t k = cidx(inx ? gi : wrapm(gi, Nx), iny ? gj : wrapm(gj, Ny), Nx);
+                hu = v.x_u[k];
+                hv = v.x_v[k];
+            }
+            su[q] = hu;
+            sv[q] = hv;
+        }
+        __syncthreads();
+        if (i < Nx && j < Ny) {
+            const size_t k = cidx(i, j, Nx);
+            const double un = su[(ty + 1) * VSX + tx + 1], vn = sv[(ty + 1) * VSX + tx + 1];
+            double au, av;
+            visc_A_any(P, make_mu(P, nullptr), TileUV{su, sv, i0, j0, Nx, Ny}, i, j, au, av);
+            const bool uf = u_fixed(P, i), vf = v_fixed(P, j);
+            const double r1 = uf ? 0.0 : v.rhs_u[k] - (un - alpha * au);
+            const double r2 = vf ? 0.0 : v.rhs_v[k] - (vn - alpha * av);
+            if (START) {  // |b|^2 of the row-eliminated system: Dirichlet rows hold their data
+                const double b1 = uf ? un : v.rhs_u[k], b2 = vf ? vn : v.rhs_v[k];
+                acc[1] += b1 * b1 + b2 * b2;
+            }
+            acc[0] += r1 * r1 + r2 * r2;
+            v.rn_u[k] = (float)r1;
+            v.rn_v[k] = (float)r2;
+            v.dn_u[k] = (float)(r1 / theta);
+            v.dn_v[k] = (float)(r2 / theta);
+            v.en_u[k] = 0.0f;
+            v.en_v[k] = 0.0f;
+        }
+        __syncthreads();
+    }
+}
+
+// ITER: CK Chebyshev steps of e, r, d on a 32x16 tile with a CK-cell halo in shared
+// memory (FP32 storage and arithmetic), the valid region shrinking by one cell per
+// step; then the tile's e, r, d and |r|^2.
+__device__ void cheb_iter(const Params& P, double alpha, double theta, double delta, double rho0, const ChebArgs& v,
+                          float* sm, double (&acc)[2]) {
+    float* eu = sm;
+    float* ev = eu + CWX * CWY;
+    float* ru = ev + CWX * CWY;
+    float* rv = ru + CWX * CWY;
+    float* du = rv + CWX * CWY;
+    float* dv = du + CWX * CWY;
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x, nthr = blockDim.x * blockDim.y;
+    const int Nx = P.g.Nx, Ny = P.g.Ny;
+    const bool px = P.g.px, py = P.g.py;
+    const double mu = P.md.viscosity_fluid;
+    const float fa = (float)alpha;
+    const float cxx = (float)(2.0 * mu * P.g.ihx * P.g.ihx), cyy = (float)(mu * P.g.ihy * P.g.ihy);
+    const float cxx2 = (float)(mu * P.g.ihx * P.g.ihx), cyy2 = (float)(2.0 * mu * P.g.ihy * P.g.ihy);
+    const float cxy = (float)(mu * P.g.ihx * P.g.ihy);
+    // per-step coefficients a_s = rho' rho, b_s = 2 rho' / delta
+    const double s1 = theta / delta;
+    float ca[CK], cb[CK];
+    {
+        double rho = rho0;
+#pragma unroll
+        for (int q = 0; q < CK; ++q) {
+            const double rn = 1.0 / (2.0 * s1 - rho);
+            ca[q] = (float)(rn * rho);
+            cb[q] = (float)(2.0 * rn / delta);
+            rho = rn;
+        }
+    }
+    const int ntx = (Nx + CTX - 1) / CTX, nt = ntx * ((Ny + CTY - 1) / CTY);
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int i0 = (t % ntx) * CTX, j0 = (t / ntx) * CTY;
+        // load the region: slots outside the grid (walls) hold 0 and are never updated
+        for (int q = tid; q < CWX * CWY; q += nthr) {
+            const int gi = i0 + q % CWX - CK, gj = j0 + q / CWX - CK;
+            const bool inx = gi >= 0 && gi < Nx, iny = gj >= 0 && gj < Ny;
+            float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, a4 = 0.f, a5 = 0.f;
+            if ((inx || px) && (iny || py)) {
+                const size_t k = cidx(inx ? gi : wrapm(gi, Nx), iny ? gj : wrapm(gj, Ny), Nx);
+                a0 = v.e_u[k]; a1 = v.e_v[k]; a2 = v.r_u[k]; a3 = v.r_v[k]; a4 = v.d_u[k]; a5 = v.d_v[k];
+            }
+            eu[q] = a0; ev[q] = a1; ru[q] = a2; rv[q] = a3; du[q] = a4; dv[q] = a5;
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int st = 0; st < CK; ++st) {
+            const int lo = st + 1, hx = CWX - 2 - st, hy = CWY - 2 - st;
+            const int w = hx - lo + 1, nreg = w * (hy - lo + 1);
+            // e += d; r -= M d with M d = d - alpha A d
+            for (int q = tid; q < nreg; q += nthr) {
+                const int lx = lo + q % w, ly = lo + q / w, sl = ly * CWX + lx;
+                const int gi = i0 + lx - CK, gj = j0 + ly - CK;
+                const bool inx = gi >= 0 && gi < Nx, iny = gj >= 0 && gj < Ny;
+                if (!((inx || px) && (iny || py))) continue;
+                const int wi = inx ? gi : wrapm(gi, Nx), wj = iny ? gj : wrapm(gj, Ny);
+                const bool uf = u_fixed(P, wi), vf = v_fixed(P, wj);
+                float au, av;
+                if ((px || (wi >= 1 && wi <= Nx - 2)) && (py || (wj >= 1 && wj <= Ny - 2))) {
+                    au = cxx * (du[sl + 1] - 2.f * du[sl] + du[sl - 1]) +
+                         cyy * (du[sl + CWX] - 2.f * du[sl] + du[sl - CWX]) +
+                         cxy * (dv[sl + CWX] - dv[sl + CWX - 1] - dv[sl] + dv[sl - 1]);
+                    av = cxx2 * (dv[sl + 1] - 2.f * dv[sl] + dv[sl - 1]) +
+                         cyy2 * (dv[sl + CWX] - 2.f * dv[sl] + dv[sl - CWX]) +
+                         cxy * (du[sl + 1] - du[sl + 1 - CWX] - du[sl] + du[sl - CWX]);
+                } else {
+                    double a1, a2;
+                    visc_A<false>(P, MuConst{mu}, ChebTile{du, dv, i0, j0, Nx, Ny}, wi, wj, a1, a2);
+                    au = (float)a1;
+                    av = (float)a2;
+                }
+                if (!uf) {
+                    eu[sl] += du[sl];
+                    ru[sl] -= du[sl] - fa * au;
+                }
+                if (!vf) {
+                    ev[sl] += dv[sl];
+                    rv[sl] -= dv[sl] - fa * av;
+                }
+            }
+            __syncthreads();
+            // d = a d + b r on the same region
+            for (int q = tid; q < nreg; q += nthr) {
+                const int lx = lo + q % w, ly = lo + q / w, sl = ly * CWX + lx;
+                du[sl] = ca[st] * du[sl] + cb[st] * ru[sl];
+                dv[sl] = ca[st] * dv[sl] + cb[st] * rv[sl];
+            }
+            __syncthreads();
+        }
+        // write the tile
+        for (int q = tid; q < CTX * CTY; q += nthr) {
+            const int lx = CK + q % CTX, ly = CK + q / CTX, sl = ly * CWX + lx;
+            const int gi = i0 + lx - CK, gj = j0 + ly - CK;
+            if (gi >= Nx || gj >= Ny) continue;
+            const size_t k = cidx(gi, gj, Nx);
+            v.en_u[k] = eu[sl]; v.en_v[k] = ev[sl];
+            v.rn_u[k] = ru[sl]; v.rn_v[k] = rv[sl];
+            v.dn_u[k] = du[sl]; v.dn_v[k] = dv[sl];
+            acc[0] += (double)ru[sl] * ru[sl] + (double)rv[sl] * rv[sl];
+        }
+        __syncthreads();
+    }
+}
+
+// The FP32 region of cheb_iter or the FP64 tile of cheb_refine.
+constexpr int kChebSmemBytes = 6 * CWX * CWY * 4 > 2 * VSX * VSY * 8 ? 6 * CWX * CWY * 4 : 2 * VSX * VSY * 8;
+
+template <bool START>
+__global__ void __launch_bounds__(VTX * VTY) k_vcheb(Params P, DtCoef ac, SolveOpts o, ChebArgs v, CGScal* cg,
+                                                     RedSlot rs, int* iters_out, cudaGraphConditionalHandle cond) {
+    __shared__ __align__(16) unsigned char smem[kChebSmemBytes];
+    __shared__ double sh[64];
+    if (!START && cg->done) return;
+    const int phase = START ? CH_REFINE : cg->phase;
+    const double alpha = ac.value();
+    double theta, delta;
+    cheb_bounds(P, alpha, theta, delta);
+    double acc[2] = {0.0, 0.0};
+    if (phase == CH_ITER) {
+        cheb_iter(P, alpha, theta, delta, cg->rho, v, reinterpret_cast<float*>(smem), acc);
+    } else if (phase == CH_APPLY) {  // x += e (pointwise)
+        const int n = P.g.Nx * P.g.Ny;
+        for (int k = (blockIdx.x * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x; k < n;
+             k += gridDim.x * blockDim.x * blockDim.y) {
+            v.x_u[k] += (double)v.e_u[k];
+            v.x_v[k] += (double)v.e_v[k];
+        }
+    } else {
+        cheb_refine<START>(P, alpha, theta, v, reinterpret_cast<double*>(smem), acc);
+    }
+    double tot[2];
+    if (grid_reduce<2>(acc, rs, tot, sh) && threadIdx.x == 0 && threadIdx.y == 0) {
+        auto next_cycle = [&](double rr) {  // start an inner cycle from a refined residual rr
+            const double drop = fmax(kChebDrop, sqrt(cg->tol2 / rr));
+            cg->nin = cheb_steps(theta, delta, drop);
+            cg->inner = 0;
+            cg->rho = delta / theta;
+            cg->phase = CH_ITER;
+        };
+        if (START) {
+            cg->rr0 = tot[0];
+            cg->rr = tot[0];
+            cg_begin(cg, o, tot[0], tot[1]);
+            if (!cg->done) next_cycle(tot[0]);
+            if (iters_out) *iters_out = 0;
+            set_loop(cond, !cg->done);
+            return;
+        }
+        cg->iter += 1;
+        if (phase == CH_ITER) {
+            double rho = cg->rho;
+            for (int q = 0; q < CK; ++q) rho = 1.0 / (2.0 * (theta / delta) - rho);
+            cg->rho = rho;
+            cg->inner += CK;
+            if (!isfinite(tot[0])) cg_unconverged(cg, tot[0]);
+            else if (cg->inner >= cg->nin) cg->phase = CH_APPLY;
+        } else if (phase == CH_APPLY) {
+            cg->phase = CH_REFINE;
+        } else {
+            cg->rr = tot[0];
+            if (tot[0] <= cg->tol2) { cg->conv = 1; cg->done = 1; }
+            else if (!isfinite(tot[0])) cg_unconverged(cg, tot[0]);
+            else next_cycle(tot[0]);
+        }
+        if (!cg->done && cg->iter >= cg->maxiter) cg_unconverged(cg, cg->rr);
+        if (iters_out) *iters_out = cg->iter;
+        set_loop(cond, !cg->done);
+    }
+}
+
+static ChebArgs cheb_args(const ViscSolve& w, const ViscMixed& m, const double* rhs_u, const double* rhs_v,
+                          int parity) {
+    const int c = parity & 1, n = c ^ 1;
+    return ChebArgs{m.r_u[c], m.r_v[c], m.w_u[c], m.w_v[c], m.s_u[c], m.s_v[c],
+                    m.r_u[n], m.r_v[n], m.w_u[n], m.w_v[n], m.s_u[n], m.s_v[n], w.x_u, w.x_v, rhs_u, rhs_v};
+}
+
+bool visc_cheb_applies(const Params& P) {
+    return P.md.viscosity == EFSI_VISC_CONSTANT && (!P.g.px || P.g.Nx >= CWX) && (!P.g.py || P.g.Ny >= CWY);
+}
+
+void visc_cheb_init(const Params& P, DtCoef alpha, const SolveOpts& o, const double* Un, const double* Vn,
+                    const double* rhs_u, const double* rhs_v, const ViscSolve& w, const ViscMixed& m, CGScal* cg,
+                    const RedSlot& rs, int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s) {
+    k_visc_x0<<<grid2(P.g.Nx, P.g.Ny), dim3(BX, BY), 0, s>>>(P, Un, Vn, w.x_u, w.x_v);
+    const int nt = ((P.g.Nx + VTX - 1) / VTX) * ((P.g.Ny + VTY - 1) / VTY);
+    // the first body launch has parity 0 and reads set 0, which START writes (its "next")
+    k_vcheb<true><<<persistent_grid(nt, P.nsm, 4), dim3(VTX, VTY), 0, s>>>(P, alpha, o, cheb_args(w, m, rhs_u, rhs_v, 1),
+                                                                         cg, rs, iters_out, cond);
+}
+
+void visc_cheb_iter(const Params& P, DtCoef alpha, const double* rhs_u, const double* rhs_v, const ViscSolve& w,
+                    const ViscMixed& m, int parity, CGScal* cg, const RedSlot& rs, int* iters_out,
+                    cudaGraphConditionalHandle cond, cudaStream_t s) {
+    const int nt = ((P.g.Nx + CTX - 1) / CTX) * ((P.g.Ny + CTY - 1) / CTY);
+    k_vcheb<false><<<persistent_grid(nt, P.nsm, 4), dim3(VTX, VTY), 0, s>>>(
+        P, alpha, SolveOpts{}, cheb_args(w, m, rhs_u, rhs_v, parity), cg, rs, iters_out, cond);
+}
+
 // NoViscosity: predictor = rhs with the Dirichlet rows enforced (:786-788).
 __global__ void k_visc_enforce(Params P, const double* __restrict__ ru, const double* __restrict__ rv, double* xu,
                                double* xv) {

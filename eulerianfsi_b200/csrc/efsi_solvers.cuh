@@ -19,7 +19,11 @@ struct CGScal {
     // (Dirichlet rows hold their data), fallback_reltol, whether the DIRECT continuation
     // is allowed / running, and the outcome (fail: relative residual fail_rel too large)
     double bnorm2, fb_tol, fail_rel;
-    int fallback, in_fallback, fail, pad;
+    int fallback, in_fallback, fail;
+    // precision form with the polynomial inner solver: Chebyshev steps of the current
+    // inner cycle (nin) and the recurrence coefficient rho of its next step
+    int nin;
+    double rho;
 };
 
 // Tolerance and iteration limit of one velocity or resource solve, from its method
@@ -89,6 +93,26 @@ void visc_mx_init(const Params& P, DtCoef alpha, const SolveOpts& o, const doubl
 void visc_mx_iter(const Params& P, DtCoef alpha, const double* phi, const double* rhs_u, const double* rhs_v,
                   const ViscSolve& w, const ViscMixed& m, int parity, CGScal* cg, const RedSlot& rs,
                   int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s);
+// Precision form for a constant viscosity: FP64 iterative refinement around an FP32
+// Chebyshev inner solver of the correction equation (I - alpha A) e = r.  The spectrum of
+// the free block lies in [1, 1 + alpha g], g the Gershgorin bound of -A, so the inner
+// iteration needs no inner products; each inner launch advances four Chebyshev steps on
+// a shared-memory tile with a four-cell halo (temporal blocking), and the refinement
+// launch applies x += e and recomputes the true FP64 residual, which alone decides
+// convergence.  Uses the FP32 arrays of ViscMixed: r and w as the ping-ponged residual
+// and direction, s as the ping-ponged correction.
+void visc_cheb_init(const Params& P, DtCoef alpha, const SolveOpts& o, const double* Un, const double* Vn,
+                    const double* rhs_u, const double* rhs_v, const ViscSolve& w, const ViscMixed& m, CGScal* cg,
+                    const RedSlot& rs, int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s);
+void visc_cheb_iter(const Params& P, DtCoef alpha, const double* rhs_u, const double* rhs_v, const ViscSolve& w,
+                    const ViscMixed& m, int parity, CGScal* cg, const RedSlot& rs, int* iters_out,
+                    cudaGraphConditionalHandle cond, cudaStream_t s);
+// Chebyshev steps per inner launch.
+constexpr int kChebSteps = 4;
+// The polynomial inner solver serves a constant viscosity on grids whose periodic
+// extents cover its shared-memory region (40 x 24 cells); other precision-form
+// configurations keep the FP32 CG of visc_mx_*.
+bool visc_cheb_applies(const Params& P);
 void visc_enforce_dirichlet(const Params& P, const double* rhs_u, const double* rhs_v, double* x_u, double* x_v,
                             cudaStream_t s);
 
