@@ -1237,6 +1237,7 @@ int efsi_create(const efsi_config* cfg, efsi_handle** out) {
         check_cuda(cudaEventCreate(&h->call_ev[1]), "event");
         Params& P = h->P;
         check_cuda(cudaDeviceGetAttribute(&P.nsm, cudaDevAttrMultiProcessorCount, h->device), "device attribute");
+        check_cuda(solvers_configure(), "solver kernel attributes");
         P.g = GridD{m.Nx, m.Ny, m.periodic_x ? 1 : 0, m.periodic_y ? 1 : 0, hx, hy, 1.0 / hx, 1.0 / hy, m.Lx, m.Ly};
         const int Nx = m.Nx, Ny = m.Ny;
         upload_bcs(h.get(), cfg->bc_U, Ny, Nx + 1, P.bu, "U");

@@ -717,7 +717,12 @@ void visc_mx_iter(const Params& P, DtCoef alpha, const double* phi, const double
 // d_0 = r_0 / theta; per step e += d, r -= M d, rho' = 1 / (2 sigma - rho),
 // d = rho' rho d + (2 rho' / delta) r.
 enum { CH_ITER = 0, CH_APPLY = 1, CH_REFINE = 2 };
-constexpr int CK = kChebSteps, CTX = 32, CTY = 16, CWX = CTX + 2 * CK, CWY = CTY + 2 * CK;
+constexpr int CK = kChebSteps, CTX = 32, CTY = 32, CWX = CTX + 2 * CK, CWY = CTY + 2 * CK;
+// Block of the body launches: CWX x CBY threads; in ITER each thread owns the CNR cells
+// (lx, ly0 + CBY m) of one region column.
+constexpr int CBY = 8, CNR = CWY / CBY, CNT = CWX * CBY, kChebBlocksPerSM = 2;
+static_assert(CWY % CBY == 0, "region rows must split evenly over the block rows");
+static_assert(CNT >= VTX * VTY, "the refinement tile needs a thread per cell");
 // Residual drop one FP32 inner cycle aims for (FP32 resolves about 1e-7).
 constexpr double kChebDrop = 1e-5;
 
@@ -769,13 +774,14 @@ template <bool START>
 __device__ void cheb_refine(const Params& P, double alpha, double theta, const ChebArgs& v, double* sm, double (&acc)[2]) {
     double* su = sm;
     double* sv = sm + VSX * VSY;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + ty * VTX;
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x, nthr = blockDim.x * blockDim.y;
+    const int tx = tid % VTX, ty = tid / VTX;  // cell of the 32x8 tile (threads past it only load)
     const int Nx = P.g.Nx, Ny = P.g.Ny;
     const int ntx = (Nx + VTX - 1) / VTX, nt = ntx * ((Ny + VTY - 1) / VTY);
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const int i0 = (t % ntx) * VTX, j0 = (t / ntx) * VTY;
         const int i = i0 + tx, j = j0 + ty;
-        for (int q = tid; q < VSX * VSY; q += VTX * VTY) {
+        for (int q = tid; q < VSX * VSY; q += nthr) {
             const int gi = i0 + q % VSX - 1, gj = j0 + q / VSX - 1;
             const bool inx = gi >= 0 && gi < Nx, iny = gj >= 0 && gj < Ny;
             double hu = 0.0, hv = 0.0;
@@ -788,7 +794,7 @@ __device__ void cheb_refine(const Params& P, double alpha, double theta, const C
             sv[q] = hv;
         }
         __syncthreads();
-        if (i < Nx && j < Ny) {
+        if (tid < VTX * VTY && i < Nx && j < Ny) {
             const size_t k = cidx(i, j, Nx);
             const double un = su[(ty + 1) * VSX + tx + 1], vn = sv[(ty + 1) * VSX + tx + 1];
             double au, av;
@@ -812,18 +818,18 @@ __device__ void cheb_refine(const Params& P, double alpha, double theta, const C
     }
 }
 
-// ITER: CK Chebyshev steps of e, r, d on a 32x16 tile with a CK-cell halo in shared
-// memory (FP32 storage and arithmetic), the valid region shrinking by one cell per
-// step; then the tile's e, r, d and |r|^2.
+// ITER: CK Chebyshev steps of e, r, d on a CTX x CTY tile with a CK-cell halo (FP32
+// storage and arithmetic).  Each thread keeps e, r and d of its CNR cells in registers
+// (e and r are pointwise); d, the only vector read at neighbours, is double-buffered in
+// shared memory, so a step is one barrier.  Every step updates the whole region but its
+// outer ring; a value next to the ring goes stale one cell per step, so after CK steps
+// the tile itself is exact.  Tiles whose region avoids walls and Dirichlet rows take the
+// constant-coefficient stencil without per-cell tests.
 __device__ void cheb_iter(const Params& P, double alpha, double theta, double delta, double rho0, const ChebArgs& v,
                           float* sm, double (&acc)[2]) {
-    float* eu = sm;
-    float* ev = eu + CWX * CWY;
-    float* ru = ev + CWX * CWY;
-    float* rv = ru + CWX * CWY;
-    float* du = rv + CWX * CWY;
-    float* dv = du + CWX * CWY;
-    const int tid = threadIdx.x + threadIdx.y * blockDim.x, nthr = blockDim.x * blockDim.y;
+    float* const dbu[2] = {sm, sm + 2 * CWX * CWY};
+    float* const dbv[2] = {sm + CWX * CWY, sm + 3 * CWX * CWY};
+    const int lx = threadIdx.x, ly0 = threadIdx.y;
     const int Nx = P.g.Nx, Ny = P.g.Ny;
     const bool px = P.g.px, py = P.g.py;
     const double mu = P.md.viscosity_fluid;
@@ -844,87 +850,148 @@ __device__ void cheb_iter(const Params& P, double alpha, double theta, double de
             rho = rn;
         }
     }
+    const bool xring = lx == 0 || lx == CWX - 1;
     const int ntx = (Nx + CTX - 1) / CTX, nt = ntx * ((Ny + CTY - 1) / CTY);
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const int i0 = (t % ntx) * CTX, j0 = (t / ntx) * CTY;
+        const bool inner = (px || (i0 - CK >= 1 && i0 + CTX + CK <= Nx - 1)) &&
+                           (py || (j0 - CK >= 1 && j0 + CTY + CK <= Ny - 1));
+        const int gi = i0 + lx - CK;
+        const bool inx = gi >= 0 && gi < Nx;
+        const int wi = inx ? gi : (px ? wrapm(gi, Nx) : 0);
+        float eu[CNR], ev[CNR], ru[CNR], rv[CNR], du[CNR], dv[CNR];
         // load the region: slots outside the grid (walls) hold 0 and are never updated
-        for (int q = tid; q < CWX * CWY; q += nthr) {
-            const int gi = i0 + q % CWX - CK, gj = j0 + q / CWX - CK;
-            const bool inx = gi >= 0 && gi < Nx, iny = gj >= 0 && gj < Ny;
-            float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, a4 = 0.f, a5 = 0.f;
+#pragma unroll
+        for (int m = 0; m < CNR; ++m) {
+            const int ly = ly0 + CBY * m, sl = ly * CWX + lx, gj = j0 + ly - CK;
+            const bool iny = gj >= 0 && gj < Ny;
+            eu[m] = ev[m] = ru[m] = rv[m] = du[m] = dv[m] = 0.f;
             if ((inx || px) && (iny || py)) {
-                const size_t k = cidx(inx ? gi : wrapm(gi, Nx), iny ? gj : wrapm(gj, Ny), Nx);
-                a0 = v.e_u[k]; a1 = v.e_v[k]; a2 = v.r_u[k]; a3 = v.r_v[k]; a4 = v.d_u[k]; a5 = v.d_v[k];
+                const size_t k = cidx(wi, iny ? gj : wrapm(gj, Ny), Nx);
+                eu[m] = v.e_u[k]; ev[m] = v.e_v[k]; ru[m] = v.r_u[k]; rv[m] = v.r_v[k]; du[m] = v.d_u[k]; dv[m] = v.d_v[k];
             }
-            eu[q] = a0; ev[q] = a1; ru[q] = a2; rv[q] = a3; du[q] = a4; dv[q] = a5;
+            dbu[0][sl] = du[m]; dbv[0][sl] = dv[m];
+            dbu[1][sl] = du[m]; dbv[1][sl] = dv[m];
         }
         __syncthreads();
+        // A d of the free interior (2 mu u_xx + mu u_yy + mu v_xy and its mirror) at slot sl
+        auto fast_A = [&](const float* cu, const float* cv, int sl, float dcu, float dcv, float& au, float& av) {
+            au = cxx * (cu[sl + 1] - 2.f * dcu + cu[sl - 1]) + cyy * (cu[sl + CWX] - 2.f * dcu + cu[sl - CWX]) +
+                 cxy * (cv[sl + CWX] - cv[sl + CWX - 1] - dcv + cv[sl - 1]);
+            av = cxx2 * (cv[sl + 1] - 2.f * dcv + cv[sl - 1]) + cyy2 * (cv[sl + CWX] - 2.f * dcv + cv[sl - CWX]) +
+                 cxy * (cu[sl + 1] - cu[sl + 1 - CWX] - dcu + cu[sl - CWX]);
+        };
+        if (inner) {  // e += d; r -= M d with M d = d - alpha A d; d = a_s d + b_s r
+#pragma unroll
+            for (int st = 0; st < CK; ++st) {
+                const float* cu = dbu[st & 1];
+                const float* cv = dbv[st & 1];
+                float* nu = dbu[(st & 1) ^ 1];
+                float* nv = dbv[(st & 1) ^ 1];
+#pragma unroll
+                for (int m = 0; m < CNR; ++m) {
+                    const int ly = ly0 + CBY * m, sl = ly * CWX + lx;
+                    if (xring || ly == 0 || ly == CWY - 1) continue;
+                    float au, av;
+                    fast_A(cu, cv, sl, du[m], dv[m], au, av);
+                    eu[m] += du[m];
+                    ru[m] -= du[m] - fa * au;
+                    du[m] = ca[st] * du[m] + cb[st] * ru[m];
+                    nu[sl] = du[m];
+                    ev[m] += dv[m];
+                    rv[m] -= dv[m] - fa * av;
+                    dv[m] = ca[st] * dv[m] + cb[st] * rv[m];
+                    nv[sl] = dv[m];
+                }
+                __syncthreads();
+            }
+        } else {
+            // tiles next to a wall or a ragged edge: per-cell tests, steps not unrolled, e
+            // and r staged in shared memory (own slots only) so that the general stencil
+            // runs with the register arrays dead
+            float* const seu = sm + 4 * CWX * CWY;
+            float* const sev = seu + CWX * CWY;
+            float* const sru = sev + CWX * CWY;
+            float* const srv = sru + CWX * CWY;
+#pragma unroll
+            for (int m = 0; m < CNR; ++m) {
+                const int sl = (ly0 + CBY * m) * CWX + lx;
+                seu[sl] = eu[m]; sev[sl] = ev[m]; sru[sl] = ru[m]; srv[sl] = rv[m];
+            }
+            double rho = rho0;
 #pragma unroll 1
-        for (int st = 0; st < CK; ++st) {
-            const int lo = st + 1, hx = CWX - 2 - st, hy = CWY - 2 - st;
-            const int w = hx - lo + 1, nreg = w * (hy - lo + 1);
-            // e += d; r -= M d with M d = d - alpha A d
-            for (int q = tid; q < nreg; q += nthr) {
-                const int lx = lo + q % w, ly = lo + q / w, sl = ly * CWX + lx;
-                const int gi = i0 + lx - CK, gj = j0 + ly - CK;
-                const bool inx = gi >= 0 && gi < Nx, iny = gj >= 0 && gj < Ny;
-                if (!((inx || px) && (iny || py))) continue;
-                const int wi = inx ? gi : wrapm(gi, Nx), wj = iny ? gj : wrapm(gj, Ny);
-                const bool uf = u_fixed(P, wi), vf = v_fixed(P, wj);
-                float au, av;
-                if ((px || (wi >= 1 && wi <= Nx - 2)) && (py || (wj >= 1 && wj <= Ny - 2))) {
-                    au = cxx * (du[sl + 1] - 2.f * du[sl] + du[sl - 1]) +
-                         cyy * (du[sl + CWX] - 2.f * du[sl] + du[sl - CWX]) +
-                         cxy * (dv[sl + CWX] - dv[sl + CWX - 1] - dv[sl] + dv[sl - 1]);
-                    av = cxx2 * (dv[sl + 1] - 2.f * dv[sl] + dv[sl - 1]) +
-                         cyy2 * (dv[sl + CWX] - 2.f * dv[sl] + dv[sl - CWX]) +
-                         cxy * (du[sl + 1] - du[sl + 1 - CWX] - du[sl] + du[sl - CWX]);
-                } else {
-                    double a1, a2;
-                    visc_A<false>(P, MuConst{mu}, ChebTile{du, dv, i0, j0, Nx, Ny}, wi, wj, a1, a2);
-                    au = (float)a1;
-                    av = (float)a2;
+            for (int st = 0; st < CK; ++st) {
+                const double rn = 1.0 / (2.0 * s1 - rho);
+                const float a_s = (float)(rn * rho), b_s = (float)(2.0 * rn / delta);
+                rho = rn;
+                const float* cu = dbu[st & 1];
+                const float* cv = dbv[st & 1];
+                float* nu = dbu[(st & 1) ^ 1];
+                float* nv = dbv[(st & 1) ^ 1];
+#pragma unroll 1
+                for (int m = 0; m < CNR; ++m) {
+                    const int ly = ly0 + CBY * m, sl = ly * CWX + lx;
+                    if (xring || ly == 0 || ly == CWY - 1) continue;
+                    const int gj = j0 + ly - CK;
+                    const bool iny = gj >= 0 && gj < Ny;
+                    if (!((inx || px) && (iny || py))) continue;
+                    const int wj = iny ? gj : wrapm(gj, Ny);
+                    const bool uf = u_fixed(P, wi), vf = v_fixed(P, wj);
+                    const float dcu = cu[sl], dcv = cv[sl];
+                    float au, av;
+                    if ((px || (wi >= 1 && wi <= Nx - 2)) && (py || (wj >= 1 && wj <= Ny - 2))) {
+                        fast_A(cu, cv, sl, dcu, dcv, au, av);
+                    } else {
+                        double a1, a2;
+                        visc_A<false>(P, MuConst{mu}, ChebTile{cu, cv, i0, j0, Nx, Ny}, wi, wj, a1, a2);
+                        au = (float)a1;
+                        av = (float)a2;
+                    }
+                    if (!uf) {
+                        const float r = sru[sl] - (dcu - fa * au);
+                        seu[sl] += dcu;
+                        sru[sl] = r;
+                        nu[sl] = a_s * dcu + b_s * r;
+                    }
+                    if (!vf) {
+                        const float r = srv[sl] - (dcv - fa * av);
+                        sev[sl] += dcv;
+                        srv[sl] = r;
+                        nv[sl] = a_s * dcv + b_s * r;
+                    }
                 }
-                if (!uf) {
-                    eu[sl] += du[sl];
-                    ru[sl] -= du[sl] - fa * au;
-                }
-                if (!vf) {
-                    ev[sl] += dv[sl];
-                    rv[sl] -= dv[sl] - fa * av;
-                }
+                __syncthreads();
             }
-            __syncthreads();
-            // d = a d + b r on the same region
-            for (int q = tid; q < nreg; q += nthr) {
-                const int lx = lo + q % w, ly = lo + q / w, sl = ly * CWX + lx;
-                du[sl] = ca[st] * du[sl] + cb[st] * ru[sl];
-                dv[sl] = ca[st] * dv[sl] + cb[st] * rv[sl];
+            // after CK steps the latest d is in buffer CK & 1 (both buffers agree elsewhere)
+#pragma unroll
+            for (int m = 0; m < CNR; ++m) {
+                const int sl = (ly0 + CBY * m) * CWX + lx;
+                eu[m] = seu[sl]; ev[m] = sev[sl]; ru[m] = sru[sl]; rv[m] = srv[sl];
+                du[m] = dbu[CK & 1][sl]; dv[m] = dbv[CK & 1][sl];
             }
-            __syncthreads();
         }
         // write the tile
-        for (int q = tid; q < CTX * CTY; q += nthr) {
-            const int lx = CK + q % CTX, ly = CK + q / CTX, sl = ly * CWX + lx;
-            const int gi = i0 + lx - CK, gj = j0 + ly - CK;
-            if (gi >= Nx || gj >= Ny) continue;
+#pragma unroll
+        for (int m = 0; m < CNR; ++m) {
+            const int ly = ly0 + CBY * m, gj = j0 + ly - CK;
+            if (lx < CK || lx >= CK + CTX || ly < CK || ly >= CK + CTY || gi >= Nx || gj >= Ny) continue;
             const size_t k = cidx(gi, gj, Nx);
-            v.en_u[k] = eu[sl]; v.en_v[k] = ev[sl];
-            v.rn_u[k] = ru[sl]; v.rn_v[k] = rv[sl];
-            v.dn_u[k] = du[sl]; v.dn_v[k] = dv[sl];
-            acc[0] += (double)ru[sl] * ru[sl] + (double)rv[sl] * rv[sl];
+            v.en_u[k] = eu[m]; v.en_v[k] = ev[m];
+            v.rn_u[k] = ru[m]; v.rn_v[k] = rv[m];
+            v.dn_u[k] = du[m]; v.dn_v[k] = dv[m];
+            acc[0] += (double)ru[m] * ru[m] + (double)rv[m] * rv[m];
         }
-        __syncthreads();
     }
 }
 
 // The FP32 region of cheb_iter or the FP64 tile of cheb_refine.
-constexpr int kChebSmemBytes = 6 * CWX * CWY * 4 > 2 * VSX * VSY * 8 ? 6 * CWX * CWY * 4 : 2 * VSX * VSY * 8;
+// (dynamic shared memory: d double-buffered plus the e, r staging of wall tiles)
+constexpr int kChebSmemBytes = 8 * CWX * CWY * 4 > 2 * VSX * VSY * 8 ? 8 * CWX * CWY * 4 : 2 * VSX * VSY * 8;
 
 template <bool START>
-__global__ void __launch_bounds__(VTX * VTY) k_vcheb(Params P, DtCoef ac, SolveOpts o, ChebArgs v, CGScal* cg,
+__global__ void __launch_bounds__(CNT, kChebBlocksPerSM) k_vcheb(Params P, DtCoef ac, SolveOpts o, ChebArgs v, CGScal* cg,
                                                      RedSlot rs, int* iters_out, cudaGraphConditionalHandle cond) {
-    __shared__ __align__(16) unsigned char smem[kChebSmemBytes];
+    extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double sh[64];
     if (!START && cg->done) return;
     const int phase = START ? CH_REFINE : cg->phase;
@@ -991,26 +1058,36 @@ static ChebArgs cheb_args(const ViscSolve& w, const ViscMixed& m, const double* 
                     m.r_u[n], m.r_v[n], m.w_u[n], m.w_v[n], m.s_u[n], m.s_v[n], w.x_u, w.x_v, rhs_u, rhs_v};
 }
 
+cudaError_t solvers_configure() {
+    cudaError_t e = cudaFuncSetAttribute(k_vcheb<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kChebSmemBytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_vcheb<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kChebSmemBytes);
+}
+
 bool visc_cheb_applies(const Params& P) {
     return P.md.viscosity == EFSI_VISC_CONSTANT && (!P.g.px || P.g.Nx >= CWX) && (!P.g.py || P.g.Ny >= CWY);
+}
+
+// One grid for every phase: a block per refinement tile (the smaller tile), at most
+// kChebBlocksPerSM per SM, which all stay resident (the launch bounds).
+static int cheb_grid(const Params& P) {
+    return persistent_grid(((P.g.Nx + VTX - 1) / VTX) * ((P.g.Ny + VTY - 1) / VTY), P.nsm, kChebBlocksPerSM);
 }
 
 void visc_cheb_init(const Params& P, DtCoef alpha, const SolveOpts& o, const double* Un, const double* Vn,
                     const double* rhs_u, const double* rhs_v, const ViscSolve& w, const ViscMixed& m, CGScal* cg,
                     const RedSlot& rs, int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s) {
     k_visc_x0<<<grid2(P.g.Nx, P.g.Ny), dim3(BX, BY), 0, s>>>(P, Un, Vn, w.x_u, w.x_v);
-    const int nt = ((P.g.Nx + VTX - 1) / VTX) * ((P.g.Ny + VTY - 1) / VTY);
     // the first body launch has parity 0 and reads set 0, which START writes (its "next")
-    k_vcheb<true><<<persistent_grid(nt, P.nsm, 4), dim3(VTX, VTY), 0, s>>>(P, alpha, o, cheb_args(w, m, rhs_u, rhs_v, 1),
-                                                                         cg, rs, iters_out, cond);
+    k_vcheb<true><<<cheb_grid(P), dim3(CWX, CBY), kChebSmemBytes, s>>>(P, alpha, o, cheb_args(w, m, rhs_u, rhs_v, 1), cg, rs,
+                                                         iters_out, cond);
 }
 
 void visc_cheb_iter(const Params& P, DtCoef alpha, const double* rhs_u, const double* rhs_v, const ViscSolve& w,
                     const ViscMixed& m, int parity, CGScal* cg, const RedSlot& rs, int* iters_out,
                     cudaGraphConditionalHandle cond, cudaStream_t s) {
-    const int nt = ((P.g.Nx + CTX - 1) / CTX) * ((P.g.Ny + CTY - 1) / CTY);
-    k_vcheb<false><<<persistent_grid(nt, P.nsm, 4), dim3(VTX, VTY), 0, s>>>(
-        P, alpha, SolveOpts{}, cheb_args(w, m, rhs_u, rhs_v, parity), cg, rs, iters_out, cond);
+    k_vcheb<false><<<cheb_grid(P), dim3(CWX, CBY), kChebSmemBytes, s>>>(P, alpha, SolveOpts{}, cheb_args(w, m, rhs_u, rhs_v, parity),
+                                                          cg, rs, iters_out, cond);
 }
 
 // NoViscosity: predictor = rhs with the Dirichlet rows enforced (:786-788).

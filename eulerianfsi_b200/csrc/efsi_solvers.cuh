@@ -113,6 +113,9 @@ constexpr int kChebSteps = 4;
 // extents cover its shared-memory region (40 x 24 cells); other precision-form
 // configurations keep the FP32 CG of visc_mx_*.
 bool visc_cheb_applies(const Params& P);
+// Function attributes of the solver kernels (dynamic shared memory); once per handle,
+// before any launch or capture.
+cudaError_t solvers_configure();
 void visc_enforce_dirichlet(const Params& P, const double* rhs_u, const double* rhs_v, double* x_u, double* x_v,
                             cudaStream_t s);
 
