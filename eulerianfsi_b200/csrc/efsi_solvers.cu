@@ -718,8 +718,9 @@ void visc_mx_iter(const Params& P, DtCoef alpha, const double* phi, const double
 // d = rho' rho d + (2 rho' / delta) r.
 enum { CH_ITER = 0, CH_APPLY = 1, CH_REFINE = 2 };
 constexpr int CK = kChebSteps, CTX = 32, CTY = 32, CWX = CTX + 2 * CK, CWY = CTY + 2 * CK;
-// Block of the body launches: CWX x CBY threads; in ITER each thread owns the CNR cells
-// (lx, ly0 + CBY m) of one region column.
+// Block of the body launches: CWX x CBY threads; in ITER thread (lx, ly0) owns the CNR
+// consecutive cells (lx, CNR ly0 + m) of one region column, so that the north and south
+// neighbours of all but its end cells are its own registers.
 constexpr int CBY = 8, CNR = CWY / CBY, CNT = CWX * CBY, kChebBlocksPerSM = 2;
 static_assert(CWY % CBY == 0, "region rows must split evenly over the block rows");
 static_assert(CNT >= VTX * VTY, "the refinement tile needs a thread per cell");
@@ -820,33 +821,46 @@ __device__ void cheb_refine(const Params& P, double alpha, double theta, const C
 
 // ITER: CK Chebyshev steps of e, r, d on a CTX x CTY tile with a CK-cell halo (FP32
 // storage and arithmetic).  Each thread keeps e, r and d of its CNR cells in registers
-// (e and r are pointwise); d, the only vector read at neighbours, is double-buffered in
-// shared memory, so a step is one barrier.  Every step updates the whole region but its
-// outer ring; a value next to the ring goes stale one cell per step, so after CK steps
-// the tile itself is exact.  Tiles whose region avoids walls and Dirichlet rows take the
-// constant-coefficient stencil without per-cell tests.
+// (e and r are pointwise); d, read at neighbours, is double-buffered in shared memory,
+// so a step is one barrier.  Free interior cells form M d = d - alpha A d directly with
+// alpha folded into the stencil weights (six shared loads per cell).  Cells next to a
+// wall or on a Dirichlet row are "special": they are listed per tile, keep e and r in
+// shared memory and are shared out over the whole block each step, so a wall tile costs
+// about as much as an interior one.  Every step updates the whole region but its outer
+// ring; a value next to the ring goes stale one cell per step, so after CK steps the
+// tile itself is exact.
 __device__ void cheb_iter(const Params& P, double alpha, double theta, double delta, double rho0, const ChebArgs& v,
                           float* sm, double (&acc)[2]) {
     float* const dbu[2] = {sm, sm + 2 * CWX * CWY};
     float* const dbv[2] = {sm + CWX * CWY, sm + 3 * CWX * CWY};
-    const int lx = threadIdx.x, ly0 = threadIdx.y;
+    float* const seu = sm + 4 * CWX * CWY;  // e, r of special cells
+    float* const sev = seu + CWX * CWY;
+    float* const sru = sev + CWX * CWY;
+    float* const srv = sru + CWX * CWY;
+    short* const slist = reinterpret_cast<short*>(srv + CWX * CWY);  // special slots of the tile
+    float* const scoef = reinterpret_cast<float*>(slist + CWX * CWY);  // a_s, b_s per step
+    __shared__ int nspec;
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x, nthr = blockDim.x * blockDim.y;
+    const int lx = threadIdx.x, lyb = CNR * threadIdx.y;
     const int Nx = P.g.Nx, Ny = P.g.Ny;
     const bool px = P.g.px, py = P.g.py;
     const double mu = P.md.viscosity_fluid;
     const float fa = (float)alpha;
-    const float cxx = (float)(2.0 * mu * P.g.ihx * P.g.ihx), cyy = (float)(mu * P.g.ihy * P.g.ihy);
-    const float cxx2 = (float)(mu * P.g.ihx * P.g.ihx), cyy2 = (float)(2.0 * mu * P.g.ihy * P.g.ihy);
-    const float cxy = (float)(mu * P.g.ihx * P.g.ihy);
-    // per-step coefficients a_s = rho' rho, b_s = 2 rho' / delta
-    const double s1 = theta / delta;
-    float ca[CK], cb[CK];
-    {
+    // M d on the free interior: kcu uC - (kx (uE + uW) + ky (uN + uS) + kxy (vN - vNW + vW - vC))
+    // and its mirror for v (2 mu u_xx + mu u_yy + mu v_xy; mu v_xx + 2 mu v_yy + mu u_xy)
+    const double ix2 = P.g.ihx * P.g.ihx, iy2 = P.g.ihy * P.g.ihy;
+    const float kx = (float)(alpha * mu * 2.0 * ix2), ky = (float)(alpha * mu * iy2);
+    const float kx2 = (float)(alpha * mu * ix2), ky2 = (float)(alpha * mu * 2.0 * iy2);
+    const float kxy = (float)(alpha * mu * P.g.ihx * P.g.ihy);
+    const float kcu = (float)(1.0 + 2.0 * alpha * mu * (2.0 * ix2 + iy2));
+    const float kcv = (float)(1.0 + 2.0 * alpha * mu * (ix2 + 2.0 * iy2));
+    if (tid == 0) {  // per-step coefficients a_s = rho' rho, b_s = 2 rho' / delta
+        const double s1 = theta / delta;
         double rho = rho0;
-#pragma unroll
         for (int q = 0; q < CK; ++q) {
             const double rn = 1.0 / (2.0 * s1 - rho);
-            ca[q] = (float)(rn * rho);
-            cb[q] = (float)(2.0 * rn / delta);
+            scoef[2 * q] = (float)(rn * rho);
+            scoef[2 * q + 1] = (float)(2.0 * rn / delta);
             rho = rn;
         }
     }
@@ -854,139 +868,132 @@ __device__ void cheb_iter(const Params& P, double alpha, double theta, double de
     const int ntx = (Nx + CTX - 1) / CTX, nt = ntx * ((Ny + CTY - 1) / CTY);
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const int i0 = (t % ntx) * CTX, j0 = (t / ntx) * CTY;
-        const bool inner = (px || (i0 - CK >= 1 && i0 + CTX + CK <= Nx - 1)) &&
-                           (py || (j0 - CK >= 1 && j0 + CTY + CK <= Ny - 1));
+        if (tid == 0) nspec = 0;
+        __syncthreads();  // also orders this tile's loads after the last tile's write-out
         const int gi = i0 + lx - CK;
         const bool inx = gi >= 0 && gi < Nx;
         const int wi = inx ? gi : (px ? wrapm(gi, Nx) : 0);
         float eu[CNR], ev[CNR], ru[CNR], rv[CNR], du[CNR], dv[CNR];
+        unsigned skip = 0;  // bit m: cell m is outside the grid, on the ring or special
         // load the region: slots outside the grid (walls) hold 0 and are never updated
 #pragma unroll
         for (int m = 0; m < CNR; ++m) {
-            const int ly = ly0 + CBY * m, sl = ly * CWX + lx, gj = j0 + ly - CK;
+            const int ly = lyb + m, sl = ly * CWX + lx, gj = j0 + ly - CK;
             const bool iny = gj >= 0 && gj < Ny;
+            const bool valid = (inx || px) && (iny || py);
             eu[m] = ev[m] = ru[m] = rv[m] = du[m] = dv[m] = 0.f;
-            if ((inx || px) && (iny || py)) {
-                const size_t k = cidx(wi, iny ? gj : wrapm(gj, Ny), Nx);
+            if (valid) {
+                const int wj = iny ? gj : wrapm(gj, Ny);
+                const size_t k = cidx(wi, wj, Nx);
                 eu[m] = v.e_u[k]; ev[m] = v.e_v[k]; ru[m] = v.r_u[k]; rv[m] = v.r_v[k]; du[m] = v.d_u[k]; dv[m] = v.d_v[k];
+                const bool ring = xring || ly == 0 || ly == CWY - 1;
+                const bool free_cell = (px || (wi >= 1 && wi <= Nx - 2)) && (py || (wj >= 1 && wj <= Ny - 2)) &&
+                                       !u_fixed(P, wi) && !v_fixed(P, wj);
+                if (ring) {
+                    skip |= 1u << m;
+                } else if (!free_cell) {
+                    skip |= 1u << m;
+                    slist[atomicAdd(&nspec, 1)] = (short)sl;
+                    seu[sl] = eu[m]; sev[sl] = ev[m]; sru[sl] = ru[m]; srv[sl] = rv[m];
+                }
+            } else {
+                skip |= 1u << m;
             }
             dbu[0][sl] = du[m]; dbv[0][sl] = dv[m];
             dbu[1][sl] = du[m]; dbv[1][sl] = dv[m];
         }
         __syncthreads();
-        // A d of the free interior (2 mu u_xx + mu u_yy + mu v_xy and its mirror) at slot sl
-        auto fast_A = [&](const float* cu, const float* cv, int sl, float dcu, float dcv, float& au, float& av) {
-            au = cxx * (cu[sl + 1] - 2.f * dcu + cu[sl - 1]) + cyy * (cu[sl + CWX] - 2.f * dcu + cu[sl - CWX]) +
-                 cxy * (cv[sl + CWX] - cv[sl + CWX - 1] - dcv + cv[sl - 1]);
-            av = cxx2 * (cv[sl + 1] - 2.f * dcv + cv[sl - 1]) + cyy2 * (cv[sl + CWX] - 2.f * dcv + cv[sl - CWX]) +
-                 cxy * (cu[sl + 1] - cu[sl + 1 - CWX] - dcu + cu[sl - CWX]);
-        };
-        if (inner) {  // e += d; r -= M d with M d = d - alpha A d; d = a_s d + b_s r
+        const int ns = nspec;
+#pragma unroll 1
+        for (int st = 0; st < CK; ++st) {
+            const float* cu = dbu[st & 1];
+            const float* cv = dbv[st & 1];
+            float* nu = dbu[(st & 1) ^ 1];
+            float* nv = dbv[(st & 1) ^ 1];
+            const float a_s = scoef[2 * st], b_s = scoef[2 * st + 1];
+            // e += d; r -= M d; d = a_s d + b_s r
+            float pu = 0.f, pv = 0.f;  // d of cell m - 1 before this step
 #pragma unroll
-            for (int st = 0; st < CK; ++st) {
-                const float* cu = dbu[st & 1];
-                const float* cv = dbv[st & 1];
-                float* nu = dbu[(st & 1) ^ 1];
-                float* nv = dbv[(st & 1) ^ 1];
+            for (int m = 0; m < CNR; ++m) {
+                const int sl = (lyb + m) * CWX + lx;
+                if (skip & (1u << m)) {  // special cells move in shared memory; refresh d
+                    du[m] = cu[sl];
+                    dv[m] = cv[sl];
+                }
+            }
 #pragma unroll
-                for (int m = 0; m < CNR; ++m) {
-                    const int ly = ly0 + CBY * m, sl = ly * CWX + lx;
-                    if (xring || ly == 0 || ly == CWY - 1) continue;
-                    float au, av;
-                    fast_A(cu, cv, sl, du[m], dv[m], au, av);
-                    eu[m] += du[m];
-                    ru[m] -= du[m] - fa * au;
-                    du[m] = ca[st] * du[m] + cb[st] * ru[m];
+            for (int m = 0; m < CNR; ++m) {
+                const int sl = (lyb + m) * CWX + lx;
+                const float uC = du[m], vC = dv[m];
+                if (!(skip & (1u << m))) {
+                    const float uS = m > 0 ? pu : cu[sl - CWX], vS = m > 0 ? pv : cv[sl - CWX];
+                    const float uN = m < CNR - 1 ? du[m + 1] : cu[sl + CWX];
+                    const float vN = m < CNR - 1 ? dv[m + 1] : cv[sl + CWX];
+                    const float uE = cu[sl + 1], uW = cu[sl - 1], vE = cv[sl + 1], vW = cv[sl - 1];
+                    const float vNW = cv[sl + CWX - 1], uSE = cu[sl + 1 - CWX];
+                    const float mdu = kcu * uC - (kx * (uE + uW) + ky * (uN + uS) + kxy * ((vN - vNW) + (vW - vC)));
+                    const float mdv = kcv * vC - (kx2 * (vE + vW) + ky2 * (vN + vS) + kxy * ((uE - uSE) + (uS - uC)));
+                    eu[m] += uC;
+                    ru[m] -= mdu;
+                    du[m] = a_s * uC + b_s * ru[m];
                     nu[sl] = du[m];
-                    ev[m] += dv[m];
-                    rv[m] -= dv[m] - fa * av;
-                    dv[m] = ca[st] * dv[m] + cb[st] * rv[m];
+                    ev[m] += vC;
+                    rv[m] -= mdv;
+                    dv[m] = a_s * vC + b_s * rv[m];
                     nv[sl] = dv[m];
                 }
-                __syncthreads();
+                pu = uC;
+                pv = vC;
             }
-        } else {
-            // tiles next to a wall or a ragged edge: per-cell tests, steps not unrolled, e
-            // and r staged in shared memory (own slots only) so that the general stencil
-            // runs with the register arrays dead
-            float* const seu = sm + 4 * CWX * CWY;
-            float* const sev = seu + CWX * CWY;
-            float* const sru = sev + CWX * CWY;
-            float* const srv = sru + CWX * CWY;
-#pragma unroll
-            for (int m = 0; m < CNR; ++m) {
-                const int sl = (ly0 + CBY * m) * CWX + lx;
-                seu[sl] = eu[m]; sev[sl] = ev[m]; sru[sl] = ru[m]; srv[sl] = rv[m];
-            }
-            double rho = rho0;
-#pragma unroll 1
-            for (int st = 0; st < CK; ++st) {
-                const double rn = 1.0 / (2.0 * s1 - rho);
-                const float a_s = (float)(rn * rho), b_s = (float)(2.0 * rn / delta);
-                rho = rn;
-                const float* cu = dbu[st & 1];
-                const float* cv = dbv[st & 1];
-                float* nu = dbu[(st & 1) ^ 1];
-                float* nv = dbv[(st & 1) ^ 1];
-#pragma unroll 1
-                for (int m = 0; m < CNR; ++m) {
-                    const int ly = ly0 + CBY * m, sl = ly * CWX + lx;
-                    if (xring || ly == 0 || ly == CWY - 1) continue;
-                    const int gj = j0 + ly - CK;
-                    const bool iny = gj >= 0 && gj < Ny;
-                    if (!((inx || px) && (iny || py))) continue;
-                    const int wj = iny ? gj : wrapm(gj, Ny);
-                    const bool uf = u_fixed(P, wi), vf = v_fixed(P, wj);
-                    const float dcu = cu[sl], dcv = cv[sl];
-                    float au, av;
-                    if ((px || (wi >= 1 && wi <= Nx - 2)) && (py || (wj >= 1 && wj <= Ny - 2))) {
-                        fast_A(cu, cv, sl, dcu, dcv, au, av);
-                    } else {
-                        double a1, a2;
-                        visc_A<false>(P, MuConst{mu}, ChebTile{cu, cv, i0, j0, Nx, Ny}, wi, wj, a1, a2);
-                        au = (float)a1;
-                        av = (float)a2;
-                    }
-                    if (!uf) {
-                        const float r = sru[sl] - (dcu - fa * au);
-                        seu[sl] += dcu;
-                        sru[sl] = r;
-                        nu[sl] = a_s * dcu + b_s * r;
-                    }
-                    if (!vf) {
-                        const float r = srv[sl] - (dcv - fa * av);
-                        sev[sl] += dcv;
-                        srv[sl] = r;
-                        nv[sl] = a_s * dcv + b_s * r;
-                    }
+            // special cells, shared out over the block: the general stencil
+            for (int q = tid; q < ns; q += nthr) {
+                const int sl = slist[q], sx = sl % CWX, sy = sl / CWX;
+                const int ci = i0 + sx - CK, cj = j0 + sy - CK;
+                const int qi = (ci >= 0 && ci < Nx) ? ci : wrapm(ci, Nx), qj = (cj >= 0 && cj < Ny) ? cj : wrapm(cj, Ny);
+                const bool uf = u_fixed(P, qi), vf = v_fixed(P, qj);
+                const float dcu = cu[sl], dcv = cv[sl];
+                double a1, a2;
+                visc_A<false>(P, MuConst{mu}, ChebTile{cu, cv, i0, j0, Nx, Ny}, qi, qj, a1, a2);
+                if (!uf) {
+                    const float r = sru[sl] - (dcu - fa * (float)a1);
+                    seu[sl] += dcu;
+                    sru[sl] = r;
+                    nu[sl] = a_s * dcu + b_s * r;
                 }
-                __syncthreads();
+                if (!vf) {
+                    const float r = srv[sl] - (dcv - fa * (float)a2);
+                    sev[sl] += dcv;
+                    srv[sl] = r;
+                    nv[sl] = a_s * dcv + b_s * r;
+                }
             }
-            // after CK steps the latest d is in buffer CK & 1 (both buffers agree elsewhere)
-#pragma unroll
-            for (int m = 0; m < CNR; ++m) {
-                const int sl = (ly0 + CBY * m) * CWX + lx;
-                eu[m] = seu[sl]; ev[m] = sev[sl]; ru[m] = sru[sl]; rv[m] = srv[sl];
-                du[m] = dbu[CK & 1][sl]; dv[m] = dbv[CK & 1][sl];
-            }
+            __syncthreads();
         }
-        // write the tile
+        // write the tile (special cells from shared memory; the latest d is in buffer CK & 1)
 #pragma unroll
         for (int m = 0; m < CNR; ++m) {
-            const int ly = ly0 + CBY * m, gj = j0 + ly - CK;
+            const int ly = lyb + m, sl = ly * CWX + lx, gj = j0 + ly - CK;
             if (lx < CK || lx >= CK + CTX || ly < CK || ly >= CK + CTY || gi >= Nx || gj >= Ny) continue;
+            float e1 = eu[m], e2 = ev[m], r1 = ru[m], r2 = rv[m], d1 = du[m], d2 = dv[m];
+            if (skip & (1u << m)) {
+                e1 = seu[sl]; e2 = sev[sl]; r1 = sru[sl]; r2 = srv[sl];
+                d1 = dbu[CK & 1][sl]; d2 = dbv[CK & 1][sl];
+            }
             const size_t k = cidx(gi, gj, Nx);
-            v.en_u[k] = eu[m]; v.en_v[k] = ev[m];
-            v.rn_u[k] = ru[m]; v.rn_v[k] = rv[m];
-            v.dn_u[k] = du[m]; v.dn_v[k] = dv[m];
-            acc[0] += (double)ru[m] * ru[m] + (double)rv[m] * rv[m];
+            v.en_u[k] = e1; v.en_v[k] = e2;
+            v.rn_u[k] = r1; v.rn_v[k] = r2;
+            v.dn_u[k] = d1; v.dn_v[k] = d2;
+            acc[0] += (double)r1 * r1 + (double)r2 * r2;
         }
     }
 }
 
 // The FP32 region of cheb_iter or the FP64 tile of cheb_refine.
-// (dynamic shared memory: d double-buffered plus the e, r staging of wall tiles)
-constexpr int kChebSmemBytes = 8 * CWX * CWY * 4 > 2 * VSX * VSY * 8 ? 8 * CWX * CWY * 4 : 2 * VSX * VSY * 8;
+// (dynamic shared memory: d double-buffered, e and r of special cells, the special-slot
+// list and the step coefficients)
+constexpr int kChebSmemBytes = 8 * CWX * CWY * 4 + CWX * CWY * 2 + 2 * CK * 4;
+static_assert(kChebSmemBytes >= 2 * VSX * VSY * 8, "the refinement tile shares the buffer");
+static_assert(CWX * CWY <= 32767, "special slots are stored as short");
 
 template <bool START>
 __global__ void __launch_bounds__(CNT, kChebBlocksPerSM) k_vcheb(Params P, DtCoef ac, SolveOpts o, ChebArgs v, CGScal* cg,
