@@ -1323,6 +1323,7 @@ int efsi_create(const efsi_config* cfg, efsi_handle** out) {
             m.p_u = h->dalloc<float>(N); m.p_v = h->dalloc<float>(N);
             m.dinv_u = h->dalloc<float>(N); m.dinv_v = h->dalloc<float>(N);
             m.rR_u = h->dalloc<float>(N); m.rR_v = h->dalloc<float>(N);
+            m.ring_w = h->dalloc<float>(visc_ring_cells(Nx, Ny) * kRingWeights);
         }
         ScalarSolve& ds = h->ds;
         ds.x = h->cs; ds.r = h->dalloc<double>(N);
@@ -1356,6 +1357,7 @@ int efsi_create(const efsi_config* cfg, efsi_handle** out) {
         std::vector<double> ones(N, 1.0);
         check_cuda(cudaMemcpy(h->sxx, ones.data(), N * sizeof(double), cudaMemcpyHostToDevice), "init");
         check_cuda(cudaMemcpy(h->syy, ones.data(), N * sizeof(double), cudaMemcpyHostToDevice), "init");
+        if (h->mixed && h->visc && visc_cheb_applies(P)) visc_ring_weights(P, h->vm.ring_w, h->stream);
         check_cuda(cudaDeviceSynchronize(), "create");
         *out = h.release();
     });

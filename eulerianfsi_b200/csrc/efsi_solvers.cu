@@ -732,7 +732,42 @@ struct ChebArgs {
     float *rn_u, *rn_v, *dn_u, *dn_v, *en_u, *en_v;  // set written by this launch
     double *x_u, *x_v;
     const double *rhs_u, *rhs_v;
+    const float* ring_w;  // A at the outer-ring cells (visc_ring_weights)
 };
+
+// Index of ring cell (i, j) in the weight table: bottom row, top row, left column,
+// right column (a corner belongs to its row).
+__device__ __forceinline__ int ring_index(const GridD& g, int i, int j) {
+    if (!g.py && j == 0) return i;
+    if (!g.py && j == g.Ny - 1) return g.Nx + i;
+    if (!g.px && i == 0) return 2 * g.Nx + j;
+    return 2 * g.Nx + g.Ny + j;
+}
+// Unit vector: 1 at component q of cell (ti, tj), 0 elsewhere.
+struct ProbeTile {
+    int q, ti, tj;
+    __device__ __forceinline__ double U(int c, int r) const { return (q == 0 && c == ti && r == tj) ? 1.0 : 0.0; }
+    __device__ __forceinline__ double V(int c, int r) const { return (q == 1 && c == ti && r == tj) ? 1.0 : 0.0; }
+};
+// One thread per (ring cell, column component, offset).
+__global__ void k_ring_weights(Params P, float* ring_w) {
+    const int Nx = P.g.Nx, Ny = P.g.Ny;
+    const int n = (int)visc_ring_cells(Nx, Ny) * 18;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int c = t / 18, rem = t % 18, q = rem / 9, dy = (rem % 9) / 3 - 1, dx = rem % 3 - 1;
+    int i, j;
+    if (c < Nx) { i = c; j = 0; }
+    else if (c < 2 * Nx) { i = c - Nx; j = Ny - 1; }
+    else if (c < 2 * Nx + Ny) { i = 0; j = c - 2 * Nx; }
+    else { i = Nx - 1; j = c - 2 * Nx - Ny; }
+    const int ti = wrapm(i + dx, Nx), tj = wrapm(j + dy, Ny);
+    double a1, a2;
+    visc_A<false>(P, MuConst{P.md.viscosity_fluid}, ProbeTile{q, ti, tj}, i, j, a1, a2);
+    float* w = ring_w + (size_t)kRingWeights * c;
+    w[9 * q + 3 * (dy + 1) + dx + 1] = (float)a1;
+    w[18 + 9 * q + 3 * (dy + 1) + dx + 1] = (float)a2;
+}
 
 // theta and delta of the free block of I - alpha A for a constant viscosity mu:
 // spec in [1, 1 + alpha g] with g = mu (max(8/hx^2 + 4/hy^2, 4/hx^2 + 8/hy^2) +
@@ -952,16 +987,25 @@ __device__ void cheb_iter(const Params& P, double alpha, double theta, double de
                 const int qi = (ci >= 0 && ci < Nx) ? ci : wrapm(ci, Nx), qj = (cj >= 0 && cj < Ny) ? cj : wrapm(cj, Ny);
                 const bool uf = u_fixed(P, qi), vf = v_fixed(P, qj);
                 const float dcu = cu[sl], dcv = cv[sl];
-                double a1, a2;
-                visc_A<false>(P, MuConst{mu}, ChebTile{cu, cv, i0, j0, Nx, Ny}, qi, qj, a1, a2);
+                const float* w = v.ring_w + (size_t)kRingWeights * ring_index(P.g, qi, qj);
+                float a1 = 0.f, a2 = 0.f;
+#pragma unroll
+                for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+                    for (int ox = 0; ox < 3; ++ox) {
+                        const int o = sl + (oy - 1) * CWX + ox - 1, k = 3 * oy + ox;
+                        const float nu_ = cu[o], nv_ = cv[o];
+                        a1 += __ldg(w + k) * nu_ + __ldg(w + 9 + k) * nv_;
+                        a2 += __ldg(w + 18 + k) * nu_ + __ldg(w + 27 + k) * nv_;
+                    }
                 if (!uf) {
-                    const float r = sru[sl] - (dcu - fa * (float)a1);
+                    const float r = sru[sl] - (dcu - fa * a1);
                     seu[sl] += dcu;
                     sru[sl] = r;
                     nu[sl] = a_s * dcu + b_s * r;
                 }
                 if (!vf) {
-                    const float r = srv[sl] - (dcv - fa * (float)a2);
+                    const float r = srv[sl] - (dcv - fa * a2);
                     sev[sl] += dcv;
                     srv[sl] = r;
                     nv[sl] = a_s * dcv + b_s * r;
@@ -1062,7 +1106,12 @@ static ChebArgs cheb_args(const ViscSolve& w, const ViscMixed& m, const double* 
                           int parity) {
     const int c = parity & 1, n = c ^ 1;
     return ChebArgs{m.r_u[c], m.r_v[c], m.w_u[c], m.w_v[c], m.s_u[c], m.s_v[c],
-                    m.r_u[n], m.r_v[n], m.w_u[n], m.w_v[n], m.s_u[n], m.s_v[n], w.x_u, w.x_v, rhs_u, rhs_v};
+                    m.r_u[n], m.r_v[n], m.w_u[n], m.w_v[n], m.s_u[n], m.s_v[n], w.x_u, w.x_v, rhs_u, rhs_v, m.ring_w};
+}
+
+void visc_ring_weights(const Params& P, float* ring_w, cudaStream_t s) {
+    const int n = (int)visc_ring_cells(P.g.Nx, P.g.Ny) * 18;
+    k_ring_weights<<<(n + 255) / 256, 256, 0, s>>>(P, ring_w);
 }
 
 cudaError_t solvers_configure() {

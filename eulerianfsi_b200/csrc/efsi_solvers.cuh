@@ -85,7 +85,17 @@ void visc_iter(const Params& P, DtCoef alpha, const double* phi, const ViscSolve
 struct ViscMixed {
     float *r_u[2], *r_v[2], *w_u[2], *w_v[2], *s_u[2], *s_v[2];
     float *p_u, *p_v, *dinv_u, *dinv_v, *rR_u, *rR_v;
+    // Constant viscosity: the viscous operator A at the cells of the grid's outer ring
+    // (walled directions) as 36 weights per cell, kRingWeights (see visc_ring_weights).
+    float* ring_w;
 };
+constexpr int kRingWeights = 36;
+// Ring cells (bottom row, top row, left column, right column): 2 Nx + 2 Ny.
+__host__ __device__ inline size_t visc_ring_cells(int Nx, int Ny) { return 2 * (size_t)Nx + 2 * (size_t)Ny; }
+// Weights of A (rows u and v at a ring cell (i, j), columns u and v at (i + dx, j + dy),
+// |dx|, |dy| <= 1) for a constant viscosity, from the general stencil probed with unit
+// vectors: ring_w[36 c + 18 o + 9 q + 3 (dy + 1) + dx + 1], o = row, q = column component.
+void visc_ring_weights(const Params& P, float* ring_w, cudaStream_t s);
 void visc_mx_init(const Params& P, DtCoef alpha, const SolveOpts& o, const double* Un, const double* Vn,
                   const double* rhs_u, const double* rhs_v, const double* phi, const ViscSolve& w,
                   const ViscMixed& m, CGScal* cg, const RedSlot& rs, int* iters_out,
