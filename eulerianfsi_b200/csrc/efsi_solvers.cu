@@ -710,13 +710,13 @@ void visc_mx_iter(const Params& P, DtCoef alpha, const double* phi, const double
 
 // ---- precision form with a constant viscosity: FP32 Chebyshev inner solver -----------
 // Phases of the body launches: ITER (kChebSteps FP32 Chebyshev steps on the correction
-// equation), APPLY (x += e in FP64), REFINE (r = rhs - (I - alpha A) x in FP64; stop or
-// start the next inner cycle from it).  Chebyshev recurrence for M e = r with
+// equation; the last launch of an inner cycle adds e to x in FP64), REFINE (r = rhs -
+// (I - alpha A) x in FP64; stop or start the next inner cycle from it).  Chebyshev recurrence for M e = r with
 // spec(M) in [1, 1 + 2 delta] (Saad, Iterative Methods for Sparse Linear Systems,
 // Algorithm 12.1): theta = 1 + delta, sigma = theta / delta, rho_0 = 1 / sigma,
 // d_0 = r_0 / theta; per step e += d, r -= M d, rho' = 1 / (2 sigma - rho),
 // d = rho' rho d + (2 rho' / delta) r.
-enum { CH_ITER = 0, CH_APPLY = 1, CH_REFINE = 2 };
+enum { CH_ITER = 0, CH_REFINE = 2 };
 constexpr int CK = kChebSteps, CTX = 32, CTY = 32, CWX = CTX + 2 * CK, CWY = CTY + 2 * CK;
 // Block of the body launches: CWX x CBY threads; in ITER thread (lx, ly0) owns the CNR
 // consecutive cells (lx, CNR ly0 + m) of one region column, so that the north and south
@@ -803,9 +803,10 @@ struct ChebTile {
     __device__ __forceinline__ double V(int c, int r) const { return sv[slot(c, r)]; }
 };
 
-// REFINE (and the START of a solve): stage x (APPLY has added the last correction) over
-// a 32x8 tile and one-cell ring, r = rhs - (x - alpha A x) in FP64 at the tile, |r|^2 and
-// |b|^2; the next inner cycle starts from r: r_set = r, d_set = r / theta, e_set = 0.
+// REFINE (and the START of a solve): stage x (the last ITER of the cycle has added the
+// correction) over a 32x8 tile and one-cell ring, r = rhs - (x - alpha A x) in FP64 at the
+// tile, |r|^2 and |b|^2; the next inner cycle starts from r: r_set = r, d_set = r / theta,
+// e_set = 0.
 template <bool START>
 __device__ void cheb_refine(const Params& P, double alpha, double theta, const ChebArgs& v, double* sm, double (&acc)[2]) {
     double* su = sm;
@@ -813,6 +814,9 @@ __device__ void cheb_refine(const Params& P, double alpha, double theta, const C
     const int tid = threadIdx.x + threadIdx.y * blockDim.x, nthr = blockDim.x * blockDim.y;
     const int tx = tid % VTX, ty = tid / VTX;  // cell of the 32x8 tile (threads past it only load)
     const int Nx = P.g.Nx, Ny = P.g.Ny;
+    const double mu = P.md.viscosity_fluid, ix2 = P.g.ihx * P.g.ihx, iy2 = P.g.ihy * P.g.ihy;
+    const double cxx = 2.0 * mu * ix2, cyy = mu * iy2, cxx2 = mu * ix2, cyy2 = 2.0 * mu * iy2;
+    const double cxy = mu * P.g.ihx * P.g.ihy;
     const int ntx = (Nx + VTX - 1) / VTX, nt = ntx * ((Ny + VTY - 1) / VTY);
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const int i0 = (t % ntx) * VTX, j0 = (t / ntx) * VTY;
@@ -832,9 +836,18 @@ __device__ void cheb_refine(const Params& P, double alpha, double theta, const C
         __syncthreads();
         if (tid < VTX * VTY && i < Nx && j < Ny) {
             const size_t k = cidx(i, j, Nx);
-            const double un = su[(ty + 1) * VSX + tx + 1], vn = sv[(ty + 1) * VSX + tx + 1];
+            const int sl = (ty + 1) * VSX + tx + 1;
+            const double un = su[sl], vn = sv[sl];
             double au, av;
-            visc_A_any(P, make_mu(P, nullptr), TileUV{su, sv, i0, j0, Nx, Ny}, i, j, au, av);
+            if ((P.g.px || (i >= 1 && i <= Nx - 2)) && (P.g.py || (j >= 1 && j <= Ny - 2))) {
+                // free interior, constant viscosity: the compact stencil read from the tile
+                au = cxx * (su[sl + 1] - 2.0 * un + su[sl - 1]) + cyy * (su[sl + VSX] - 2.0 * un + su[sl - VSX]) +
+                     cxy * (sv[sl + VSX] - sv[sl + VSX - 1] - vn + sv[sl - 1]);
+                av = cxx2 * (sv[sl + 1] - 2.0 * vn + sv[sl - 1]) + cyy2 * (sv[sl + VSX] - 2.0 * vn + sv[sl - VSX]) +
+                     cxy * (su[sl + 1] - su[sl + 1 - VSX] - un + su[sl - VSX]);
+            } else {
+                visc_A<false>(P, MuConst{mu}, TileUV{su, sv, i0, j0, Nx, Ny}, i, j, au, av);
+            }
             const bool uf = u_fixed(P, i), vf = v_fixed(P, j);
             const double r1 = uf ? 0.0 : v.rhs_u[k] - (un - alpha * au);
             const double r2 = vf ? 0.0 : v.rhs_v[k] - (vn - alpha * av);
@@ -864,8 +877,8 @@ __device__ void cheb_refine(const Params& P, double alpha, double theta, const C
 // about as much as an interior one.  Every step updates the whole region but its outer
 // ring; a value next to the ring goes stale one cell per step, so after CK steps the
 // tile itself is exact.
-__device__ void cheb_iter(const Params& P, double alpha, double theta, double delta, double rho0, const ChebArgs& v,
-                          float* sm, double (&acc)[2]) {
+__device__ void cheb_iter(const Params& P, double alpha, double theta, double delta, double rho0, bool last,
+                          const ChebArgs& v, float* sm, double (&acc)[2]) {
     float* const dbu[2] = {sm, sm + 2 * CWX * CWY};
     float* const dbv[2] = {sm + CWX * CWY, sm + 3 * CWX * CWY};
     float* const seu = sm + 4 * CWX * CWY;  // e, r of special cells
@@ -1024,9 +1037,14 @@ __device__ void cheb_iter(const Params& P, double alpha, double theta, double de
                 d1 = dbu[CK & 1][sl]; d2 = dbv[CK & 1][sl];
             }
             const size_t k = cidx(gi, gj, Nx);
-            v.en_u[k] = e1; v.en_v[k] = e2;
-            v.rn_u[k] = r1; v.rn_v[k] = r2;
-            v.dn_u[k] = d1; v.dn_v[k] = d2;
+            if (last) {  // end of the inner cycle: x += e (REFINE then restarts r, d, e)
+                v.x_u[k] += (double)e1;
+                v.x_v[k] += (double)e2;
+            } else {
+                v.en_u[k] = e1; v.en_v[k] = e2;
+                v.rn_u[k] = r1; v.rn_v[k] = r2;
+                v.dn_u[k] = d1; v.dn_v[k] = d2;
+            }
             acc[0] += (double)r1 * r1 + (double)r2 * r2;
         }
     }
@@ -1051,14 +1069,7 @@ __global__ void __launch_bounds__(CNT, kChebBlocksPerSM) k_vcheb(Params P, DtCoe
     cheb_bounds(P, alpha, theta, delta);
     double acc[2] = {0.0, 0.0};
     if (phase == CH_ITER) {
-        cheb_iter(P, alpha, theta, delta, cg->rho, v, reinterpret_cast<float*>(smem), acc);
-    } else if (phase == CH_APPLY) {  // x += e (pointwise)
-        const int n = P.g.Nx * P.g.Ny;
-        for (int k = (blockIdx.x * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x; k < n;
-             k += gridDim.x * blockDim.x * blockDim.y) {
-            v.x_u[k] += (double)v.e_u[k];
-            v.x_v[k] += (double)v.e_v[k];
-        }
+        cheb_iter(P, alpha, theta, delta, cg->rho, cg->inner + CK >= cg->nin, v, reinterpret_cast<float*>(smem), acc);
     } else {
         cheb_refine<START>(P, alpha, theta, v, reinterpret_cast<double*>(smem), acc);
     }
@@ -1087,9 +1098,7 @@ __global__ void __launch_bounds__(CNT, kChebBlocksPerSM) k_vcheb(Params P, DtCoe
             cg->rho = rho;
             cg->inner += CK;
             if (!isfinite(tot[0])) cg_unconverged(cg, tot[0]);
-            else if (cg->inner >= cg->nin) cg->phase = CH_APPLY;
-        } else if (phase == CH_APPLY) {
-            cg->phase = CH_REFINE;
+            else if (cg->inner >= cg->nin) cg->phase = CH_REFINE;
         } else {
             cg->rr = tot[0];
             if (tot[0] <= cg->tol2) { cg->conv = 1; cg->done = 1; }
