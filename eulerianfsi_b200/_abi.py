@@ -33,6 +33,7 @@ EXT_NONE, EXT_IDENTITY_OUTSIDE, EXT_GEOMETRIC = range(3)
 PRECISION_FP64, PRECISION_MIXED = range(2)
 LINEAR_DIRECT, LINEAR_GMRES = range(2)
 LINEAR_HARD_CAP = 10000
+PROJECTION_AUTO, PROJECTION_MULTIGRID = range(2)
 STEP_GRAPH, STEP_HOST = range(2)
 
 _dp = POINTER(c_double)
@@ -83,7 +84,8 @@ class Numerics(Structure):
         ("check_stage1_constraint", c_int32),
         ("linear_reltol", c_double), ("linear_maxiter", c_int32),
         ("precision", c_int32), ("velocity_method", c_int32), ("resource_method", c_int32),
-        ("direct_fallback", c_int32), ("fallback_reltol", c_double), ("reserved", c_int32 * 4),
+        ("direct_fallback", c_int32), ("fallback_reltol", c_double), ("projection_solver", c_int32),
+        ("reserved", c_int32 * 3),
     ]
 
 
@@ -153,7 +155,7 @@ class Diagnostics(Structure):
 
 
 SITES = ["phase", "momentum", "structure", "visc_apply", "visc_cg", "visc_init", "pcg_matvec",
-         "pcg_update", "vcycle", "proj_rhs", "proj_finish", "combine", "vel_rhs", "finalize"]
+         "pcg_update", "vcycle", "proj_rhs", "proj_finish", "combine", "vel_rhs", "finalize", "spectral"]
 
 
 # Entry points shared by the CUDA library (prefix "efsi_") and the CPU oracle

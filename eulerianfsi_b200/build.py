@@ -21,7 +21,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libefsi.so")
 STAMP = OUT + ".stamp"
-SOURCES = ["efsi_solvers.cu", "efsi_ops.cu", "efsi_adjoint.cu", "efsi_phase.cu", "efsi_diag.cu", "efsi_api.cu"]
+SOURCES = ["efsi_solvers.cu", "efsi_spectral.cu", "efsi_ops.cu", "efsi_adjoint.cu", "efsi_phase.cu", "efsi_diag.cu",
+           "efsi_api.cu"]
 HEADERS = ["efsi_common.cuh", "efsi_device.cuh", "efsi_kernels.cuh", "efsi_solvers.cuh", "efsi_diag.cuh",
            "efsi_adjoint.cuh"]
 PUBLIC_HEADER = os.path.join(os.path.dirname(HERE), "include", "efsi.h")

@@ -459,6 +459,88 @@ std::vector<double> coarse_inverse(const HostLevel& L, double ax, double ay, boo
     return inv;
 }
 
+// The 1-D kind of one direction of level 0 (SPEC_*), or -1 when the boundary factors of
+// a side are not uniform (a mixed side) or the size is not a power of two.
+int spectral_kind(bool periodic, const std::vector<double>& lo, const std::vector<double>& hi, int n) {
+    if (n < 2 || (n & (n - 1)) != 0) return -1;
+    if (periodic) return SPEC_P;
+    auto uniform = [](const std::vector<double>& c) {
+        for (double v : c)
+            if (v != c[0]) return false;
+        return c[0] == 0.0 || c[0] == 2.0;
+    };
+    if (!uniform(lo) || !uniform(hi)) return -1;
+    const bool dl = lo[0] == 2.0, dr = hi[0] == 2.0;
+    return dl ? (dr ? SPEC_DD : SPEC_DN) : (dr ? SPEC_ND : SPEC_NN);
+}
+
+// Twiddles and eigenvalues of one direction (long double host trigonometry).
+SpecDir spectral_dir(efsi_handle* h, int kind, int n) {
+    SpecDir d{};
+    d.n = n;
+    d.kind = kind;
+    d.L = (kind == SPEC_ND || kind == SPEC_DN) ? 2 * n : n;
+    d.logL = 0;
+    while ((1 << d.logL) < d.L) ++d.logL;
+    const long double pi = 3.141592653589793238462643383279502884L;
+    std::vector<double2> w(std::max(1, d.L / 2)), mk(d.L);
+    for (int t = 0; t < d.L / 2; ++t) {
+        const long double a = 2.0L * pi * t / d.L;
+        w[t] = make_double2((double)cosl(a), (double)-sinl(a));
+    }
+    for (int k = 0; k < d.L; ++k) {
+        const long double a = pi * k / (2.0L * d.L);
+        mk[k] = make_double2((double)cosl(a), (double)-sinl(a));
+    }
+    std::vector<double> mu(n);
+    for (int k = 0; k < n; ++k) {
+        long double v;
+        switch (kind) {
+            case SPEC_NN: v = 2.0L - 2.0L * cosl(pi * k / n); break;
+            case SPEC_DD: v = 2.0L + 2.0L * cosl(pi * k / n); break;
+            case SPEC_ND: case SPEC_DN: v = 2.0L - 2.0L * cosl(pi * (2 * k + 1) / (2.0L * n)); break;
+            default: v = 2.0L - 2.0L * cosl(2.0L * pi * k / n); break;
+        }
+        mu[k] = k == 0 && (kind == SPEC_NN || kind == SPEC_P) ? 0.0 : (double)v;
+    }
+    auto upload = [&](const auto& v) {
+        using T = typename std::decay_t<decltype(v)>::value_type;
+        T* p = h->dalloc<T>(v.size());
+        check_cuda(cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "spectral upload");
+        return p;
+    };
+    d.w = upload(w);
+    d.mk = upload(mk);
+    d.mu = upload(mu);
+    return d;
+}
+
+// Enable the direct projection solve when both directions allow it and the per-block
+// shared memory (FFT buffer + a tile of rows) fits.
+void setup_spectral(efsi_handle* h, const HostLevel& L0, bool px, bool py) {
+    Spectral& sp = h->pj.sp;
+    sp = Spectral{};
+    const int kx = spectral_kind(px, L0.cl, L0.cr, L0.nx), ky = spectral_kind(py, L0.cb, L0.ct, L0.ny);
+    if (kx < 0 || ky < 0) return;
+    const int Lx = (kx == SPEC_ND || kx == SPEC_DN) ? 2 * L0.nx : L0.nx;
+    const int Ly = (ky == SPEC_ND || ky == SPEC_DN) ? 2 * L0.ny : L0.ny;
+    constexpr size_t kBudget = 200 * 1024;
+    auto rows = [&](int L, int n) {
+        const size_t fft = 16 * (size_t)L, row = 8 * (size_t)n;
+        if (fft + row > kBudget) return 0;
+        return (int)std::min<size_t>(4, (kBudget - fft) / row);
+    };
+    sp.rows_a = rows(Lx, L0.nx);
+    sp.rows_b = rows(Ly, L0.ny);
+    if (sp.rows_a < 1 || sp.rows_b < 1) return;
+    sp.smem_a = 16 * (size_t)Lx + 8 * (size_t)sp.rows_a * L0.nx;
+    sp.smem_b = 16 * (size_t)Ly + 8 * (size_t)sp.rows_b * L0.ny;
+    sp.dx = spectral_dir(h, kx, L0.nx);
+    sp.dy = spectral_dir(h, ky, L0.ny);
+    sp.on = true;
+    check_cuda(spectral_configure(sp), "spectral kernel attributes");
+}
+
 void build_projection(efsi_handle* h, const efsi_config& cfg) {
     const int Nx = h->Nx, Ny = h->Ny;
     const bool px = cfg.mesh.periodic_x, py = cfg.mesh.periodic_y;
@@ -521,6 +603,7 @@ void build_projection(efsi_handle* h, const efsi_config& cfg) {
     pj.Ap = h->dalloc<double>(N); pj.b = h->dalloc<double>(N); pj.rhs = h->dalloc<double>(N);
     pj.w = h->dalloc<double>(N); pj.s[0] = h->dalloc<double>(N); pj.s[1] = h->dalloc<double>(N);
     pj.Up = h->dalloc<double>(h->nu); pj.Vp = h->dalloc<double>(h->nv);
+    if (cfg.numerics.projection_solver == EFSI_PROJECTION_AUTO) setup_spectral(h, L0, px, py);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -677,6 +760,21 @@ void proj_solve(efsi_handle* h, int stage_slot, double reltol, const double* q0)
     const Params& P = h->P;
     DevBlock* d = h->dev;
     const double N = (double)h->nc;
+    if (h->pj.sp.on) {  // direct fast-diagonalisation solve inside a Richardson iteration
+        solve(
+            h, KIND_PROJ, stage_slot, &d->cg_proj, P.nu.projection_maxiter, 3, 1,
+            [&](cudaStream_t s, int* io, cudaGraphConditionalHandle ch) {
+                proj_spectral_init(P, h->pj, reltol, P.nu.projection_maxiter, q0, &d->cg_proj, &d->ps, h->slot[1],
+                                   &d->st, io, ch, s);
+                h->launches += 1;
+            },
+            [&](cudaStream_t s, int* io, cudaGraphConditionalHandle ch) {
+                // residual + x transform (2 x 8 N B), y pass (2 x 8 N), x pass + update (3 x 8 N)
+                site(h, EFSI_SITE_SPECTRAL, 8.0 * N * 9.0,
+                     [&] { proj_spectral_iter(P, h->pj, &d->cg_proj, &d->ps, h->slot[4], io, ch, s); });
+            });
+        return;
+    }
     const double vb = proj_update_vcycle_bytes(h->pj);
     const int vk = proj_update_vcycle_kernels(h->pj);
     solve(

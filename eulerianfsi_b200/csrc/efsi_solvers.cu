@@ -2145,6 +2145,14 @@ void proj_cg_init(const Params& P, const Projection& pj, double reltol, int maxi
     vcycle(pj, pj.r[0], nullptr, cg, rs, rs2, nullptr, 0, P.g.px, P.g.py, s);
 }
 
+void proj_spectral_init(const Params& P, const Projection& pj, double reltol, int maxiter, const double* q0,
+                        CGScal* cg, const ProjScal* ps, const RedSlot& rs, const DevStatus* st, int* iters_out,
+                        cudaGraphConditionalHandle cond, cudaStream_t s) {
+    const MGLevel& L = pj.lev[0];
+    k_pcg_init<<<persistent_grid(tiles2(L.nx, L.ny), P.nsm, 6), dim3(BX, BY), 0, s>>>(
+        L, P.g.px, P.g.py, reltol, maxiter, q0, pj.b, pj.x, pj.r[0], ps, cg, rs, st, iters_out, cond);
+}
+
 // One CG iteration is proj_matvec then proj_update_vcycle with the same parity:
 // p[parity] is written, r[parity] is read and r[parity^1] written (multigrid case).
 void proj_matvec(const Params& P, const Projection& pj, int parity, CGScal* cg, const RedSlot& rs, cudaStream_t s) {

@@ -147,9 +147,28 @@ struct MGLevel {
     double *x, *xo, *b, *r;             // level vectors (x/xo ping-pong)
     float *xf, *xof, *bf;               // the same in FP32 (precision form)
 };
+// Fast diagonalisation of the level-0 operator K = ax (Tx (x) I) + ay (I (x) Ty) when
+// both 1-D operators have one boundary kind per side and power-of-two sizes: Tx, Ty are
+// diagonalised by a cosine, sine or Hartley transform computed with a complex FFT.
+enum SpecKind : int { SPEC_NN = 0, SPEC_DD = 1, SPEC_ND = 2, SPEC_DN = 3, SPEC_P = 4 };
+struct SpecDir {
+    int n;              // cells along the direction
+    int L, logL;        // complex FFT length (n, or 2n for the odd extension of ND / DN)
+    int kind;           // SpecKind
+    const double2* w;   // exp(-2 pi i t / L), t < L / 2
+    const double2* mk;  // exp(-i pi k / (2 L)), k < L (cosine-transform twiddles)
+    const double* mu;   // eigenvalues of the 1-D operator, n
+};
+struct Spectral {
+    bool on;
+    SpecDir dx, dy;
+    int rows_a, rows_b;  // rows (x pass) and modes (y pass) per block
+    size_t smem_a, smem_b;
+};
 struct Projection {
     int nlev;
     MGLevel lev[16];
+    Spectral sp;          // direct solve of level 0 (used instead of multigrid CG when on)
     double* coarse_inv;   // dense inverse of the coarsest operator (shifted when singular)
     float* coarse_inv_f;  // its FP32 copy (precision form)
     int nc;
@@ -183,6 +202,17 @@ void proj_update_vcycle(const Params& P, const Projection& pj, int parity, CGSca
 void proj_finish(const Params& P, const Projection& pj, const double* G, double* q_out, double* U_out,
                  double* V_out, ProjScal* ps, double* stage_linf, const RedSlot& rs1, const RedSlot& rs2,
                  DevStatus* st, cudaStream_t s);
+// Richardson iteration with the exact spectral inverse, x += K^-1 (b - K x), from the
+// initial guess and tolerance that proj_cg_init set (no V-cycle is run): one body is
+// three kernels (residual and x transform; y transform, eigenvalue division and inverse;
+// inverse x transform and update).  Configuring the kernels' shared memory happens in
+// spectral_configure (before any capture).
+void proj_spectral_init(const Params& P, const Projection& pj, double reltol, int maxiter, const double* q0,
+                        CGScal* cg, const ProjScal* ps, const RedSlot& rs, const DevStatus* st, int* iters_out,
+                        cudaGraphConditionalHandle cond, cudaStream_t s);
+void proj_spectral_iter(const Params& P, const Projection& pj, CGScal* cg, const ProjScal* ps, const RedSlot& rs,
+                        int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s);
+cudaError_t spectral_configure(const Spectral& sp);
 // ps->v[6] = mean of the solution pj.x with a constant nullspace (0 otherwise).
 void proj_mean(const Params& P, const Projection& pj, ProjScal* ps, const RedSlot& rs, cudaStream_t s);
 // Kernel launches of proj_update_vcycle and of proj_cg_init (statistics).

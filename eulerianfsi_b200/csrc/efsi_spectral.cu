@@ -1,0 +1,261 @@
+// efsi_spectral.cu — direct solve of the projection's Poisson problem by fast
+// diagonalisation (Lynch, Rice and Thomas, "Direct solution of partial difference
+// equations by tensor product methods", Numer. Math. 6, 1964).
+//
+// On a uniform grid the level-0 operator of the projection (cell-area weighted -L,
+// Projection.jl:106-113 for the matrix) is K = ax (Tx (x) I) + ay (I (x) Ty), with Tx,
+// Ty the 1-D second-difference operators whose end rows carry the boundary kind of each
+// side (Neumann: 1, Dirichlet: 3, periodic: wrap).  Each 1-D operator is diagonalised by
+// a real transform, evaluated with a power-of-two complex FFT in shared memory:
+//   Neumann-Neumann      DCT-II (Makhoul, IEEE Trans. ASSP 28, 1980: even/odd reorder,
+//                        one complex FFT of length n, a post-twiddle)   mu = 2 - 2 cos(pi k / n)
+//   Dirichlet-Dirichlet  DCT-II of (-1)^i x (DST-II with reversed modes) mu = 2 + 2 cos(pi k / n)
+//   Neumann-Dirichlet    odd extension about the Dirichlet face, DCT-II of length 2n, odd modes
+//                        (DCT-IV)                                        mu = 2 - 2 cos(pi (2k+1) / 2n)
+//   Dirichlet-Neumann    the same on the reversed index
+//   periodic             Hartley transform (Re F - Im F)                  mu = 2 - 2 cos(2 pi k / n)
+// so K^-1 = Fx^-1 Fy^-1 diag(1 / (ax mu_x + ay mu_y)) Fy Fx (the zero mode of a singular
+// operator is dropped: the zero-mean solution).  The solve is used as the exact inverse
+// of a Richardson iteration x += K^-1 (b - K x) judged by the FP64 residual, so the
+// projection's relative tolerance keeps its meaning; one iteration reaches about 1e-13.
+//
+// Data flow of one iteration (three launches, the arrays stay L2-resident at 1024^2):
+//   A  rows j: r = (b - mean) - K x (FP64, |r|^2 decides convergence), x transform of r,
+//      modes written transposed (T[j + k Ny]);
+//   B  modes k: y transform, division by the eigenvalue, inverse y transform, written
+//      transposed back (T2[k + j Nx]);
+//   C  rows j: inverse x transform, x += e.
+#include "efsi_solvers.cuh"
+
+namespace efsi {
+
+namespace {
+
+constexpr int kSpecThreads = 256;
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ int brev(int i, int logL) { return (int)(__brev((unsigned)i) >> (32 - logL)); }
+
+// In-place radix-2 decimation-in-time FFT (forward sign) of a[0, L); the input is stored
+// in bit-reversed order.  Every thread of the block takes part; ends with a barrier.
+__device__ void fft_smem(double2* a, const SpecDir& d) {
+    const int L = d.L;
+    for (int s = 1; s <= d.logL; ++s) {
+        const int h = 1 << (s - 1), ts = L >> s;
+        for (int q = threadIdx.x; q < L / 2; q += blockDim.x) {
+            const int j = q & (h - 1), i0 = ((q >> (s - 1)) << s) + j, i1 = i0 + h;
+            const double2 t = cmul(__ldg(d.w + j * ts), a[i1]), u = a[i0];
+            a[i0] = make_double2(u.x + t.x, u.y + t.y);
+            a[i1] = make_double2(u.x - t.x, u.y - t.y);
+        }
+        __syncthreads();
+    }
+}
+
+// Position of input e (0 <= e < L) in the bit-reversed FFT input of the Makhoul DCT-II:
+// v_m = x_2m, v_(L-1-m) = x_(2m+1).
+__device__ __forceinline__ int dct_slot(int e, const SpecDir& d) {
+    const int p = (e & 1) ? d.L - 1 - (e >> 1) : (e >> 1);
+    return brev(p, d.logL);
+}
+
+// Forward transform, scatter of input value x at index i (0 <= i < n).
+__device__ __forceinline__ void fwd_put(double2* a, const SpecDir& d, int i, double x) {
+    switch (d.kind) {
+    case SPEC_NN: a[dct_slot(i, d)] = make_double2(x, 0.0); break;
+    case SPEC_DD: a[dct_slot(i, d)] = make_double2((i & 1) ? -x : x, 0.0); break;
+    case SPEC_ND:
+        a[dct_slot(i, d)] = make_double2(x, 0.0);
+        a[dct_slot(d.L - 1 - i, d)] = make_double2(-x, 0.0);
+        break;
+    case SPEC_DN: {
+        const int m = d.n - 1 - i;
+        a[dct_slot(m, d)] = make_double2(x, 0.0);
+        a[dct_slot(d.L - 1 - m, d)] = make_double2(-x, 0.0);
+        break;
+    }
+    default: a[brev(i, d.logL)] = make_double2(x, 0.0); break;  // SPEC_P
+    }
+}
+// Forward transform, mode k (0 <= k < n) after the FFT.
+__device__ __forceinline__ double fwd_get(const double2* a, const SpecDir& d, int k) {
+    if (d.kind == SPEC_P) return a[k].x - a[k].y;
+    const int kk = (d.kind == SPEC_ND || d.kind == SPEC_DN) ? 2 * k + 1 : k;
+    const double2 m = __ldg(d.mk + kk), v = a[kk];
+    return m.x * v.x - m.y * v.y;  // Re(exp(-i pi kk / 2L) V_kk)
+}
+// Inverse transform, FFT input at index k (0 <= k < L) from the modes X(.) (0 <= . < n):
+// the DCT-II inverse of Makhoul, conj(V_k) = exp(-i pi k / 2L) (X_k + i X_(L-k)), X_L = 0,
+// with X the odd-mode embedding for ND / DN; the Hartley transform for periodic.
+template <class G>
+__device__ __forceinline__ void inv_put(double2* a, const SpecDir& d, int k, const G& X) {
+    double2 c;
+    if (d.kind == SPEC_P) {
+        c = make_double2(X(k), 0.0);
+    } else {
+        double xk, xnk;
+        if (d.kind == SPEC_ND || d.kind == SPEC_DN) {
+            if (k & 1) { xk = X((k - 1) >> 1); xnk = X((d.L - k - 1) >> 1); }
+            else { xk = 0.0; xnk = 0.0; }
+        } else {
+            xk = X(k);
+            xnk = k == 0 ? 0.0 : X(d.L - k);
+        }
+        const double2 m = __ldg(d.mk + k);
+        c = make_double2(m.x * xk - m.y * xnk, m.x * xnk + m.y * xk);
+    }
+    a[brev(k, d.logL)] = c;
+}
+// Inverse transform, output value at index i (0 <= i < n) after the FFT.
+__device__ __forceinline__ double inv_get(const double2* a, const SpecDir& d, int i) {
+    if (d.kind == SPEC_P) return (a[i].x - a[i].y) / d.n;
+    const int e = d.kind == SPEC_DN ? d.n - 1 - i : i;
+    const int p = (e & 1) ? d.L - 1 - (e >> 1) : (e >> 1);
+    const double v = a[p].x / d.L;
+    return (d.kind == SPEC_DD && (i & 1)) ? -v : v;
+}
+
+// K x at cell (i, j) of level 0 (the weighted operator with its boundary factors).
+__device__ __forceinline__ double apply_K(const MGLevel& L, int px, int py, const double* x, int i, int j) {
+    const int nx = L.nx, ny = L.ny;
+    const size_t k = cidx(i, j, nx);
+    double d = 0.0, off = 0.0;
+    if (i > 0) { d += L.ax; off += L.ax * x[k - 1]; }
+    else if (px) { d += L.ax; off += L.ax * x[k + nx - 1]; }
+    else d += L.ax * L.cl[j];
+    if (i < nx - 1) { d += L.ax; off += L.ax * x[k + 1]; }
+    else if (px) { d += L.ax; off += L.ax * x[k - (nx - 1)]; }
+    else d += L.ax * L.cr[j];
+    if (j > 0) { d += L.ay; off += L.ay * x[k - nx]; }
+    else if (py) { d += L.ay; off += L.ay * x[k + (size_t)(ny - 1) * nx]; }
+    else d += L.ay * L.cb[i];
+    if (j < ny - 1) { d += L.ay; off += L.ay * x[k + nx]; }
+    else if (py) { d += L.ay; off += L.ay * x[k - (size_t)(ny - 1) * nx]; }
+    else d += L.ay * L.ct[i];
+    return d * x[k] - off;
+}
+
+// A: residual and x transform of rows j0 .. j0 + rows_a - 1; convergence decision.
+__global__ void __launch_bounds__(kSpecThreads) k_spec_a(Spectral sp, MGLevel L0, int px, int py,
+                                                        const double* __restrict__ b, const double* __restrict__ x,
+                                                        double* __restrict__ T, const ProjScal* ps, CGScal* cg,
+                                                        RedSlot rs, int* iters_out, cudaGraphConditionalHandle cond) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double sh[32];
+    if (cg->done) return;
+    const SpecDir& d = sp.dx;
+    double2* a = reinterpret_cast<double2*>(smem);
+    double* tile = reinterpret_cast<double*>(a + d.L);
+    const int nx = L0.nx, ny = L0.ny, R = sp.rows_a, j0 = blockIdx.x * R;
+    const double bmean = ps->v[10];
+    double acc[1] = {0.0};
+    for (int r = 0; r < R; ++r) {
+        const int j = j0 + r;
+        if (j >= ny) break;  // uniform over the block
+        for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+            const double v = (b[cidx(i, j, nx)] - bmean) - apply_K(L0, px, py, x, i, j);
+            acc[0] += v * v;
+            fwd_put(a, d, i, v);
+        }
+        __syncthreads();
+        fft_smem(a, d);
+        for (int k = threadIdx.x; k < nx; k += blockDim.x) tile[r * nx + k] = fwd_get(a, d, k);
+        __syncthreads();
+    }
+    for (int q = threadIdx.x; q < R * nx; q += blockDim.x) {
+        const int k = q / R, r = q % R, j = j0 + r;
+        if (j < ny) T[(size_t)j + (size_t)k * ny] = tile[r * nx + k];
+    }
+    double tot[1];
+    if (grid_reduce<1>(acc, rs, tot, sh) && threadIdx.x == 0) {
+        cg->rr = tot[0];
+        if (tot[0] <= cg->tol2) { cg->conv = 1; cg->done = 1; }
+        else if (cg->iter >= cg->maxiter || !isfinite(tot[0])) cg->done = 1;
+        if (iters_out) *iters_out = cg->iter;
+        set_loop(cond, !cg->done);
+    }
+}
+
+// B: y transform of modes k0 .. k0 + rows_b - 1, division, inverse y transform.
+__global__ void __launch_bounds__(kSpecThreads) k_spec_b(Spectral sp, double ax, double ay,
+                                                        const double* __restrict__ T, double* __restrict__ T2,
+                                                        const CGScal* cg) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (cg->done) return;
+    const SpecDir& dx = sp.dx;
+    const SpecDir& d = sp.dy;
+    double2* a = reinterpret_cast<double2*>(smem);
+    double* tile = reinterpret_cast<double*>(a + d.L);
+    const int nx = dx.n, ny = d.n, R = sp.rows_b, k0 = blockIdx.x * R;
+    for (int r = 0; r < R; ++r) {
+        const int k = k0 + r;
+        if (k >= nx) break;  // uniform over the block
+        double* row = tile + (size_t)r * ny;
+        for (int l = threadIdx.x; l < ny; l += blockDim.x) fwd_put(a, d, l, T[(size_t)k * ny + l]);
+        __syncthreads();
+        fft_smem(a, d);
+        const double mx = ax * __ldg(dx.mu + k);
+        for (int l = threadIdx.x; l < ny; l += blockDim.x) {
+            const double lam = mx + ay * __ldg(d.mu + l);
+            row[l] = lam > 0.0 ? fwd_get(a, d, l) / lam : 0.0;
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < d.L; q += blockDim.x) inv_put(a, d, q, [&](int m) { return row[m]; });
+        __syncthreads();
+        fft_smem(a, d);
+        for (int l = threadIdx.x; l < ny; l += blockDim.x) row[l] = inv_get(a, d, l);
+        __syncthreads();
+    }
+    for (int q = threadIdx.x; q < R * ny; q += blockDim.x) {
+        const int l = q / R, r = q % R, k = k0 + r;
+        if (k < nx) T2[(size_t)k + (size_t)l * nx] = tile[(size_t)r * ny + l];
+    }
+}
+
+// C: inverse x transform of row j, x += e; the iteration count.
+__global__ void __launch_bounds__(kSpecThreads) k_spec_c(Spectral sp, const double* __restrict__ T2, double* x,
+                                                        CGScal* cg, int* iters_out) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (cg->done) return;
+    const SpecDir& d = sp.dx;
+    double2* a = reinterpret_cast<double2*>(smem);
+    const int nx = d.n, j = blockIdx.x;
+    const double* row = T2 + (size_t)j * nx;
+    for (int q = threadIdx.x; q < d.L; q += blockDim.x) inv_put(a, d, q, [&](int m) { return row[m]; });
+    __syncthreads();
+    fft_smem(a, d);
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) x[cidx(i, j, nx)] += inv_get(a, d, i);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        cg->iter += 1;
+        if (iters_out) *iters_out = cg->iter;
+    }
+}
+
+}  // namespace
+
+cudaError_t spectral_configure(const Spectral& sp) {
+    if (!sp.on) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(k_spec_a, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.smem_a);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_spec_b, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.smem_b);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_spec_c, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(16 * (size_t)sp.dx.L));
+    return e;
+}
+
+void proj_spectral_iter(const Params& P, const Projection& pj, CGScal* cg, const ProjScal* ps, const RedSlot& rs,
+                        int* iters_out, cudaGraphConditionalHandle cond, cudaStream_t s) {
+    const Spectral& sp = pj.sp;
+    const MGLevel& L = pj.lev[0];
+    const int ga = (L.ny + sp.rows_a - 1) / sp.rows_a, gb = (L.nx + sp.rows_b - 1) / sp.rows_b;
+    // T = pj.z (modes, y contiguous), T2 = pj.w (modes, x contiguous)
+    k_spec_a<<<ga, kSpecThreads, sp.smem_a, s>>>(sp, L, P.g.px, P.g.py, pj.b, pj.x, pj.z, ps, cg, rs, iters_out,
+                                                  cond);
+    k_spec_b<<<gb, kSpecThreads, sp.smem_b, s>>>(sp, L.ax, L.ay, pj.z, pj.w, cg);
+    k_spec_c<<<L.ny, kSpecThreads, 16 * (size_t)sp.dx.L, s>>>(sp, pj.w, pj.x, cg, iters_out);
+}
+
+}  // namespace efsi

@@ -271,8 +271,10 @@ def build_imex_context(metrics: MeshMetrics, bcs: FSIBoundaryConditions, models:
                        numerics: IMEXNumerics | None = None, use_projection_amg: bool = True,
                        backend: str = "cuda") -> IMEXContext:
     """build_imex_context (TimeIntegrationIMEX.jl:468-493) with the device backend.
-    `use_projection_amg` is accepted for signature compatibility; the device always
-    preconditions the projection with geometric multigrid."""
+    `use_projection_amg` is accepted for signature compatibility; the device solves the
+    projection with its own solvers (`IMEXNumerics.projection_solver`: the direct
+    fast-diagonalisation solve where the grid allows it, multigrid-preconditioned CG
+    otherwise)."""
     numerics = numerics if numerics is not None else IMEXNumerics()
     if backend != "cuda":
         raise ArgumentError("the only backend of this library is 'cuda'")

@@ -446,9 +446,13 @@ class LinearSolverOptions:
 
 @dataclass(frozen=True)
 class IMEXNumerics:
-    """IMEXNumerics (TimeIntegrationIMEX.jl:262-301) plus the device precision form
-    (``precision="fp64"`` for the plain step, ``"mixed"`` for FP32 stencil bulk and
-    multigrid with FP64 state, residuals, inner products and refinement)."""
+    """IMEXNumerics (TimeIntegrationIMEX.jl:262-301) plus two device options of this
+    library: the precision form (``precision="fp64"`` for the plain step, ``"mixed"`` for
+    FP32 solver bulk with FP64 state, residuals, inner products and refinement) and the
+    projection solver (``projection_solver="auto"``: the direct fast-diagonalisation
+    solve where the grid has power-of-two sizes and one boundary kind per side of the
+    correction potential, the multigrid CG elsewhere; ``"multigrid"``: always the CG).
+    Both projection solvers stop on the relative residual ``projection_reltol``."""
     scheme: FourStageIMEXFractionalStep = field(default_factory=FourStageIMEXFractionalStep)
     linear_solvers: LinearSolverOptions = field(default_factory=LinearSolverOptions)
     structure_extension: AbstractStructureExtension = field(default_factory=NoStructureExtension)
@@ -459,6 +463,7 @@ class IMEXNumerics:
     stage1_constraint_rtol: float = 1e-8
     check_stage1_constraint: bool = True
     precision: str = "fp64"
+    projection_solver: str = "auto"
 
     def __post_init__(self):
         if not self.projection_reltol > 0:
@@ -473,6 +478,8 @@ class IMEXNumerics:
             raise ArgumentError("stage1_constraint_rtol must be non-negative.")
         if self.precision not in ("fp64", "mixed"):
             raise ArgumentError("precision must be 'fp64' or 'mixed'.")
+        if self.projection_solver not in ("auto", "multigrid"):
+            raise ArgumentError("projection_solver must be 'auto' or 'multigrid'.")
 
 
 # ---- flattening into the C structs ------------------------------------------------
@@ -609,3 +616,5 @@ def fill_numerics(out: _abi.Numerics, n: IMEXNumerics) -> None:
     out.direct_fallback = int(bool(ls.direct_fallback))
     out.fallback_reltol = ls.fallback_reltol
     out.precision = _abi.PRECISION_MIXED if n.precision == "mixed" else _abi.PRECISION_FP64
+    out.projection_solver = (_abi.PROJECTION_MULTIGRID if n.projection_solver == "multigrid"
+                             else _abi.PROJECTION_AUTO)

@@ -166,6 +166,12 @@ typedef struct efsi_models {
 #define EFSI_LINEAR_DIRECT          0
 #define EFSI_LINEAR_GMRES           1
 #define EFSI_LINEAR_HARD_CAP        10000
+/* Projection solver: AUTO takes the direct fast-diagonalisation solve when the grid
+ * allows it (power-of-two sizes, one boundary kind per side of the correction potential)
+ * and the multigrid-preconditioned CG otherwise; MULTIGRID always takes the CG.  Both
+ * stop on the same relative residual (projection_reltol). */
+#define EFSI_PROJECTION_AUTO      0
+#define EFSI_PROJECTION_MULTIGRID 1
 
 typedef struct efsi_numerics {
     int32_t structure_extension;  double extension_rate, extension_exponent, extension_cutoff;
@@ -178,7 +184,8 @@ typedef struct efsi_numerics {
     int32_t resource_method;      /* EFSI_LINEAR_*                                             */
     int32_t direct_fallback;      /* options.direct_fallback                                   */
     double  fallback_reltol;      /* options.fallback_reltol                                   */
-    int32_t reserved[4];
+    int32_t projection_solver;    /* EFSI_PROJECTION_* (an extension of this library)          */
+    int32_t reserved[3];
 } efsi_numerics;
 
 typedef struct efsi_config {
@@ -227,7 +234,8 @@ typedef struct efsi_projection_result {
 #define EFSI_SITE_COMBINE        11   /* stage combination of phi, sigma, c              */
 #define EFSI_SITE_VEL_RHS        12   /* viscous predictor right-hand side               */
 #define EFSI_SITE_FINALIZE       13   /* state commit + StepReport reductions            */
-#define EFSI_SITE_COUNT          14
+#define EFSI_SITE_SPECTRAL       14   /* projection direct solve: one refinement pass     */
+#define EFSI_SITE_COUNT          15
 
 /* Solver statistics and device timings of the most recent call. */
 typedef struct efsi_stats {

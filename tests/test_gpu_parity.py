@@ -157,10 +157,16 @@ def test_viscous_operator(case):
     assert rel_err(outs[0], outs[1]) <= OP_TOL
 
 
+SPECTRAL_CASES = ("cavity_256", "periodic", "channel")  # power-of-two sizes, one boundary kind per side
+
+
+@pytest.mark.parametrize("solver", ["auto", "multigrid"])
 @pytest.mark.parametrize("case", ["cavity_neumann", "cavity_256", "dirichlet", "periodic", "periodic_224", "channel"])
-def test_projection(case):
-    """Projection parity; the multigrid preconditioner restates the oracle's V-cycle,
-    so the CG iteration counts agree as well (ragged tiles: 48, 40; several levels: 256, 224)."""
+def test_projection(case, solver):
+    """Projection parity.  With the multigrid CG the preconditioner restates the oracle's
+    V-cycle, so the CG iteration counts agree as well (ragged tiles: 48, 40; several
+    levels: 256, 224).  The direct solve (auto on power-of-two grids with one boundary
+    kind per side) converges in one or two refinement passes."""
     if case in ("cavity_neumann", "cavity_256"):
         w = workloads.cavity_disk(N=48 if case == "cavity_neumann" else 256)
         metrics, bcs, models, numerics = w.metrics, w.bcs, w.models, tight(w.numerics)
@@ -178,6 +184,8 @@ def test_projection(case):
         nb = ef.BoundaryConditionSetup(n0, n0, n0, n0)
         bcs = ef.FSIBoundaryConditions(nb, nb, bq, nb, {"xx": nb, "yy": nb, "xy": nb})
         models, numerics = ef.FSIModels(), ef.IMEXNumerics(projection_reltol=1e-13)
+    import dataclasses
+    numerics = dataclasses.replace(numerics, projection_solver=solver)
     gpu, ora = pair(metrics, bcs, models, numerics)
     inp = random_inputs(metrics, seed=13)
     Nx, Ny = metrics.Nx, metrics.Ny
@@ -199,7 +207,62 @@ def test_projection(case):
     assert rel_err(U1, U2) <= 1e-10 and rel_err(V1, V2) <= 1e-10
     assert rel_err(q1, q2) <= 1e-10
     assert r1.constraint_linf <= 1e-9 and r2.constraint_linf <= 1e-9
-    assert it1 > 0 and abs(it1 - it2) <= 1, (it1, it2)
+    if solver == "auto" and case in SPECTRAL_CASES:
+        assert 1 <= it1 <= 2, it1
+    else:
+        assert it1 > 0 and abs(it1 - it2) <= 1, (it1, it2)
+
+
+def _kind_setup(kind, n):
+    """(periodic, low side, high side) of the correction potential for one direction."""
+    d0, n0 = ef.Dirichlet(0.0), ef.Neumann(0.0)
+    return {"NN": (False, n0, n0), "DD": (False, d0, d0), "ND": (False, n0, d0), "DN": (False, d0, n0),
+            "P": (True, ef.Periodic(), ef.Periodic())}[kind]
+
+
+@pytest.mark.parametrize("kinds", [("NN", "DD"), ("DD", "ND"), ("DN", "NN"), ("P", "DD"), ("ND", "P"), ("DN", "DN")])
+def test_projection_direct_solve_kinds(kinds):
+    """Every 1-D transform of the direct projection solve (cosine for Neumann sides,
+    sign-flipped cosine for Dirichlet, odd extension for one Dirichlet side, Hartley for
+    periodic) against the oracle's CG and the device multigrid CG, on a 64 x 32 grid."""
+    import dataclasses
+    Nx, Ny = 64, 32
+    (pxx, xl, xr), (pyy, yb, yt) = _kind_setup(kinds[0], Nx), _kind_setup(kinds[1], Ny)
+    grid = ef.generate_grid(2.0, 1.0, Nx, Ny)
+    metrics = ef.build_mesh_metrics(grid, periodic_x=pxx, periodic_y=pyy)
+    n0, p = ef.Neumann(0.0), ef.Periodic()
+    vel = ef.BoundaryConditionSetup(p if pxx else n0, p if pxx else n0, p if pyy else n0, p if pyy else n0)
+    bq = ef.BoundaryConditionSetup(xl, xr, yb, yt)
+    bcs = ef.FSIBoundaryConditions(vel, vel, bq, vel, {"xx": vel, "yy": vel, "xy": vel})
+    models = ef.FSIModels()
+    inp = random_inputs(metrics, seed=17)
+    if pxx:
+        inp["U"][-1, :] = inp["U"][0, :]
+    if pyy:
+        inp["V"][:, -1] = inp["V"][:, 0]
+    singular = all(k in ("NN", "P") for k in kinds)
+    G = fz(Nx, Ny) if singular else inp["G"]
+    if singular and not (pxx and pyy):
+        if not pxx:
+            inp["U"][0, :] = inp["U"][-1, :] = 0.0
+        if not pyy:
+            inp["V"][:, 0] = inp["V"][:, -1] = 0.0
+    out = {}
+    for label, solver in (("direct", "auto"), ("multigrid", "multigrid")):
+        numerics = ef.IMEXNumerics(projection_reltol=1e-13, projection_solver=solver)
+        gpu, ora = pair(metrics, bcs, models, numerics)
+        for name, h in (("gpu_" + label, gpu), ("oracle", ora)):
+            U, V = inp["U"].copy(order="F"), inp["V"].copy(order="F")
+            h.set_correction(fz(Nx, Ny))
+            r = _abi.ProjectionResultC()
+            h.call("project", dp(U), dp(V), dp(G), C.byref(r))
+            out[name] = (U, V, h.get_correction(), r, h.stats()["projection_iterations"][0])
+    for name in ("gpu_direct", "gpu_multigrid"):
+        for a, b in zip(out[name][:3], out["oracle"][:3]):
+            assert rel_err(a, b) <= 1e-10, (name, rel_err(a, b))
+        assert out[name][3].constraint_linf <= 1e-9
+    assert 1 <= out["gpu_direct"][4] <= 2, out["gpu_direct"][4]
+    assert out["gpu_multigrid"][4] > 2
 
 
 def test_projection_incompatible_source_raises():
@@ -285,15 +348,25 @@ def test_channel_growth_steps():
     assert rg[-1].minimum_resource > 0 and rg[-1].maximum_growth_trace_error >= 0.0
 
 
-def test_reference_growth_smoke_on_gpu():
-    """test/growth_tests.jl:96-142 through the CUDA library."""
+@pytest.mark.parametrize("solver", ["multigrid", "auto"])
+def test_reference_growth_smoke_on_gpu(solver):
+    """test/growth_tests.jl:96-142 through the CUDA library.  The problem is uniform in x,
+    so the compatible velocity is vertical: U vanishes in exact arithmetic, and the
+    reference's `maximum(abs, state.U) > 0` holds through the rounding of its solver.
+    It is restated for the multigrid CG (which leaves such rounding too); the direct
+    solve keeps the x-uniformity exactly, so there the outflow is checked on V and U is
+    checked to vanish."""
     from tests.test_oracle_known_answers import growth_smoke_problem
     grid, metrics, bcs, models, state = growth_smoke_problem()
-    ctx = ef.build_imex_context(metrics, bcs, models, use_projection_amg=False)
+    ctx = ef.build_imex_context(metrics, bcs, models, numerics=ef.IMEXNumerics(projection_solver=solver),
+                                use_projection_amg=False)
     work = ef.allocate_imex_workspace(metrics)
     res = ef.make_velocity_compatible(state, ctx, work)
     assert res.constraint_linf < 1e-7
-    assert np.max(np.abs(state.U)) > 0.0
+    if solver == "multigrid":
+        assert np.max(np.abs(state.U)) > 0.0
+    else:
+        assert np.max(np.abs(state.V)) > 0.0 and np.max(np.abs(state.U)) < 1e-12
     work.correction[...] = 0.0
     rep = ef.integrate_step(state, 0.0, 1e-4, ctx, work)
     assert rep.maximum_projection_constraint_linf < 1e-6
