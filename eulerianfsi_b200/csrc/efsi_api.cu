@@ -524,17 +524,24 @@ void setup_spectral(efsi_handle* h, const HostLevel& L0, bool px, bool py) {
     if (kx < 0 || ky < 0) return;
     const int Lx = (kx == SPEC_ND || kx == SPEC_DN) ? 2 * L0.nx : L0.nx;
     const int Ly = (ky == SPEC_ND || ky == SPEC_DN) ? 2 * L0.ny : L0.ny;
-    constexpr size_t kBudget = 200 * 1024;
-    auto rows = [&](int L, int n) {
-        const size_t fft = 16 * (size_t)L, row = 8 * (size_t)n;
-        if (fft + row > kBudget) return 0;
-        return (int)std::min<size_t>(4, (kBudget - fft) / row);
+    // per block: L/2 twiddles, R padded FFT rows and (A, B) an R x n tile of modes; at
+    // most four rows, and at most ~112 KB so that two blocks share an SM
+    constexpr size_t kBudget = 112 * 1024, kMax = 220 * 1024;
+    auto smem = [](int L, int n, int R, bool tile) {
+        return 16 * (size_t)(L / 2) + 16 * (size_t)R * spectral_row(L) + (tile ? 8 * (size_t)R * n : 0);
     };
-    sp.rows_a = rows(Lx, L0.nx);
-    sp.rows_b = rows(Ly, L0.ny);
-    if (sp.rows_a < 1 || sp.rows_b < 1) return;
-    sp.smem_a = 16 * (size_t)Lx + 8 * (size_t)sp.rows_a * L0.nx;
-    sp.smem_b = 16 * (size_t)Ly + 8 * (size_t)sp.rows_b * L0.ny;
+    auto rows = [&](int L, int n, bool tile) {
+        int R = 4;
+        while (R > 1 && smem(L, n, R, tile) > kBudget) --R;
+        return smem(L, n, R, tile) <= kMax ? R : 0;
+    };
+    sp.rows_a = rows(Lx, L0.nx, true);
+    sp.rows_b = rows(Ly, L0.ny, true);
+    sp.rows_c = rows(Lx, L0.nx, false);
+    if (sp.rows_a < 1 || sp.rows_b < 1 || sp.rows_c < 1) return;
+    sp.smem_a = smem(Lx, L0.nx, sp.rows_a, true);
+    sp.smem_b = smem(Ly, L0.ny, sp.rows_b, true);
+    sp.smem_c = smem(Lx, L0.nx, sp.rows_c, false);
     sp.dx = spectral_dir(h, kx, L0.nx);
     sp.dy = spectral_dir(h, ky, L0.ny);
     sp.on = true;

@@ -162,9 +162,11 @@ struct SpecDir {
 struct Spectral {
     bool on;
     SpecDir dx, dy;
-    int rows_a, rows_b;  // rows (x pass) and modes (y pass) per block
-    size_t smem_a, smem_b;
+    int rows_a, rows_b, rows_c;  // rows (x passes) and modes (y pass) transformed per block
+    size_t smem_a, smem_b, smem_c;
 };
+// Padded complex elements of one FFT row of length L in shared memory (one spare per 32).
+__host__ __device__ inline int spectral_row(int L) { return L + (L >> 5); }
 struct Projection {
     int nlev;
     MGLevel lev[16];

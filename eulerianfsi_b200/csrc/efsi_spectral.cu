@@ -37,18 +37,34 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 __device__ __forceinline__ int brev(int i, int logL) { return (int)(__brev((unsigned)i) >> (32 - logL)); }
+// Padded shared-memory slot of FFT element i (one spare element per 32, so that the
+// bit-reversed scatters and the butterflies of a warp spread over the banks).
+__device__ __forceinline__ int pad(int i) { return i + (i >> 5); }
 
-// In-place radix-2 decimation-in-time FFT (forward sign) of a[0, L); the input is stored
-// in bit-reversed order.  Every thread of the block takes part; ends with a barrier.
-__device__ void fft_smem(double2* a, const SpecDir& d) {
-    const int L = d.L;
+// Shared-memory layout of one block: the L/2 twiddles, then R FFT rows of spectral_row(L)
+// padded elements (R rows are transformed at once, with the same barriers as one).
+__device__ __forceinline__ double2* fft_rows(unsigned char* smem, const SpecDir& d) {
+    return reinterpret_cast<double2*>(smem) + d.L / 2;
+}
+__device__ __forceinline__ void load_twiddles(unsigned char* smem, const SpecDir& d) {
+    double2* tw = reinterpret_cast<double2*>(smem);
+    for (int t = threadIdx.x; t < d.L / 2; t += blockDim.x) tw[t] = __ldg(d.w + t);
+}
+
+// In-place radix-2 decimation-in-time FFT (forward sign) of R rows a[r * stride + pad(.)]
+// whose inputs are stored in bit-reversed order; ends with a barrier.
+__device__ void fft_smem(double2* a, const double2* tw, const SpecDir& d, int R) {
+    const int L = d.L, half = L / 2, stride = spectral_row(L);
     for (int s = 1; s <= d.logL; ++s) {
         const int h = 1 << (s - 1), ts = L >> s;
-        for (int q = threadIdx.x; q < L / 2; q += blockDim.x) {
-            const int j = q & (h - 1), i0 = ((q >> (s - 1)) << s) + j, i1 = i0 + h;
-            const double2 t = cmul(__ldg(d.w + j * ts), a[i1]), u = a[i0];
-            a[i0] = make_double2(u.x + t.x, u.y + t.y);
-            a[i1] = make_double2(u.x - t.x, u.y - t.y);
+        for (int q = threadIdx.x; q < R * half; q += blockDim.x) {
+            const int r = q / half, qq = q - r * half;
+            const int j = qq & (h - 1), i0 = ((qq >> (s - 1)) << s) + j;
+            double2* row = a + (size_t)r * stride;
+            const int p0 = pad(i0), p1 = pad(i0 + h);
+            const double2 t = cmul(tw[j * ts], row[p1]), u = row[p0];
+            row[p0] = make_double2(u.x + t.x, u.y + t.y);
+            row[p1] = make_double2(u.x - t.x, u.y - t.y);
         }
         __syncthreads();
     }
@@ -58,10 +74,10 @@ __device__ void fft_smem(double2* a, const SpecDir& d) {
 // v_m = x_2m, v_(L-1-m) = x_(2m+1).
 __device__ __forceinline__ int dct_slot(int e, const SpecDir& d) {
     const int p = (e & 1) ? d.L - 1 - (e >> 1) : (e >> 1);
-    return brev(p, d.logL);
+    return pad(brev(p, d.logL));
 }
 
-// Forward transform, scatter of input value x at index i (0 <= i < n).
+// Forward transform, scatter of input value x at index i (0 <= i < n) into one row.
 __device__ __forceinline__ void fwd_put(double2* a, const SpecDir& d, int i, double x) {
     switch (d.kind) {
     case SPEC_NN: a[dct_slot(i, d)] = make_double2(x, 0.0); break;
@@ -76,19 +92,23 @@ __device__ __forceinline__ void fwd_put(double2* a, const SpecDir& d, int i, dou
         a[dct_slot(d.L - 1 - m, d)] = make_double2(-x, 0.0);
         break;
     }
-    default: a[brev(i, d.logL)] = make_double2(x, 0.0); break;  // SPEC_P
+    default: a[pad(brev(i, d.logL))] = make_double2(x, 0.0); break;  // SPEC_P
     }
 }
-// Forward transform, mode k (0 <= k < n) after the FFT.
+// Forward transform, mode k (0 <= k < n) of one row after the FFT.
 __device__ __forceinline__ double fwd_get(const double2* a, const SpecDir& d, int k) {
-    if (d.kind == SPEC_P) return a[k].x - a[k].y;
+    if (d.kind == SPEC_P) {
+        const double2 v = a[pad(k)];
+        return v.x - v.y;
+    }
     const int kk = (d.kind == SPEC_ND || d.kind == SPEC_DN) ? 2 * k + 1 : k;
-    const double2 m = __ldg(d.mk + kk), v = a[kk];
+    const double2 m = __ldg(d.mk + kk), v = a[pad(kk)];
     return m.x * v.x - m.y * v.y;  // Re(exp(-i pi kk / 2L) V_kk)
 }
-// Inverse transform, FFT input at index k (0 <= k < L) from the modes X(.) (0 <= . < n):
-// the DCT-II inverse of Makhoul, conj(V_k) = exp(-i pi k / 2L) (X_k + i X_(L-k)), X_L = 0,
-// with X the odd-mode embedding for ND / DN; the Hartley transform for periodic.
+// Inverse transform, FFT input at index k (0 <= k < L) of one row from the modes X(.)
+// (0 <= . < n): the DCT-II inverse of Makhoul, conj(V_k) = exp(-i pi k / 2L) (X_k + i
+// X_(L-k)), X_L = 0, with X the odd-mode embedding for ND / DN; the Hartley transform for
+// periodic.
 template <class G>
 __device__ __forceinline__ void inv_put(double2* a, const SpecDir& d, int k, const G& X) {
     double2 c;
@@ -106,14 +126,17 @@ __device__ __forceinline__ void inv_put(double2* a, const SpecDir& d, int k, con
         const double2 m = __ldg(d.mk + k);
         c = make_double2(m.x * xk - m.y * xnk, m.x * xnk + m.y * xk);
     }
-    a[brev(k, d.logL)] = c;
+    a[pad(brev(k, d.logL))] = c;
 }
-// Inverse transform, output value at index i (0 <= i < n) after the FFT.
+// Inverse transform, output value at index i (0 <= i < n) of one row after the FFT.
 __device__ __forceinline__ double inv_get(const double2* a, const SpecDir& d, int i) {
-    if (d.kind == SPEC_P) return (a[i].x - a[i].y) / d.n;
+    if (d.kind == SPEC_P) {
+        const double2 v = a[pad(i)];
+        return (v.x - v.y) / d.n;
+    }
     const int e = d.kind == SPEC_DN ? d.n - 1 - i : i;
     const int p = (e & 1) ? d.L - 1 - (e >> 1) : (e >> 1);
-    const double v = a[p].x / d.L;
+    const double v = a[pad(p)].x / d.L;
     return (d.kind == SPEC_DD && (i & 1)) ? -v : v;
 }
 
@@ -137,7 +160,8 @@ __device__ __forceinline__ double apply_K(const MGLevel& L, int px, int py, cons
     return d * x[k] - off;
 }
 
-// A: residual and x transform of rows j0 .. j0 + rows_a - 1; convergence decision.
+// A: residual and x transform of rows j0 .. j0 + R - 1 (transformed together); the
+// modes go to the tile and from there transposed to T; convergence decision.
 __global__ void __launch_bounds__(kSpecThreads) k_spec_a(Spectral sp, MGLevel L0, int px, int py,
                                                         const double* __restrict__ b, const double* __restrict__ x,
                                                         double* __restrict__ T, const ProjScal* ps, CGScal* cg,
@@ -146,27 +170,30 @@ __global__ void __launch_bounds__(kSpecThreads) k_spec_a(Spectral sp, MGLevel L0
     __shared__ double sh[32];
     if (cg->done) return;
     const SpecDir& d = sp.dx;
-    double2* a = reinterpret_cast<double2*>(smem);
-    double* tile = reinterpret_cast<double*>(a + d.L);
-    const int nx = L0.nx, ny = L0.ny, R = sp.rows_a, j0 = blockIdx.x * R;
+    const double2* tw = reinterpret_cast<const double2*>(smem);
+    double2* a = fft_rows(smem, d);
+    const int stride = spectral_row(d.L);
+    const int nx = L0.nx, ny = L0.ny, j0 = blockIdx.x * sp.rows_a, R = min(sp.rows_a, ny - j0);
+    double* tile = reinterpret_cast<double*>(a + (size_t)sp.rows_a * stride);
     const double bmean = ps->v[10];
+    load_twiddles(smem, d);
     double acc[1] = {0.0};
-    for (int r = 0; r < R; ++r) {
-        const int j = j0 + r;
-        if (j >= ny) break;  // uniform over the block
-        for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-            const double v = (b[cidx(i, j, nx)] - bmean) - apply_K(L0, px, py, x, i, j);
-            acc[0] += v * v;
-            fwd_put(a, d, i, v);
-        }
-        __syncthreads();
-        fft_smem(a, d);
-        for (int k = threadIdx.x; k < nx; k += blockDim.x) tile[r * nx + k] = fwd_get(a, d, k);
-        __syncthreads();
-    }
     for (int q = threadIdx.x; q < R * nx; q += blockDim.x) {
-        const int k = q / R, r = q % R, j = j0 + r;
-        if (j < ny) T[(size_t)j + (size_t)k * ny] = tile[r * nx + k];
+        const int r = q / nx, i = q - r * nx, j = j0 + r;
+        const double v = (b[cidx(i, j, nx)] - bmean) - apply_K(L0, px, py, x, i, j);
+        acc[0] += v * v;
+        fwd_put(a + (size_t)r * stride, d, i, v);
+    }
+    __syncthreads();
+    fft_smem(a, tw, d, R);
+    for (int q = threadIdx.x; q < R * nx; q += blockDim.x) {
+        const int r = q / nx, k = q - r * nx;
+        tile[q] = fwd_get(a + (size_t)r * stride, d, k);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < R * nx; q += blockDim.x) {
+        const int k = q / R, r = q - k * R;
+        T[(size_t)(j0 + r) + (size_t)k * ny] = tile[r * nx + k];
     }
     double tot[1];
     if (grid_reduce<1>(acc, rs, tot, sh) && threadIdx.x == 0) {
@@ -178,7 +205,8 @@ __global__ void __launch_bounds__(kSpecThreads) k_spec_a(Spectral sp, MGLevel L0
     }
 }
 
-// B: y transform of modes k0 .. k0 + rows_b - 1, division, inverse y transform.
+// B: y transform of modes k0 .. k0 + R - 1 (together), division by the eigenvalue,
+// inverse y transform, written transposed to T2.
 __global__ void __launch_bounds__(kSpecThreads) k_spec_b(Spectral sp, double ax, double ay,
                                                         const double* __restrict__ T, double* __restrict__ T2,
                                                         const CGScal* cg) {
@@ -186,47 +214,64 @@ __global__ void __launch_bounds__(kSpecThreads) k_spec_b(Spectral sp, double ax,
     if (cg->done) return;
     const SpecDir& dx = sp.dx;
     const SpecDir& d = sp.dy;
-    double2* a = reinterpret_cast<double2*>(smem);
-    double* tile = reinterpret_cast<double*>(a + d.L);
-    const int nx = dx.n, ny = d.n, R = sp.rows_b, k0 = blockIdx.x * R;
-    for (int r = 0; r < R; ++r) {
-        const int k = k0 + r;
-        if (k >= nx) break;  // uniform over the block
-        double* row = tile + (size_t)r * ny;
-        for (int l = threadIdx.x; l < ny; l += blockDim.x) fwd_put(a, d, l, T[(size_t)k * ny + l]);
-        __syncthreads();
-        fft_smem(a, d);
-        const double mx = ax * __ldg(dx.mu + k);
-        for (int l = threadIdx.x; l < ny; l += blockDim.x) {
-            const double lam = mx + ay * __ldg(d.mu + l);
-            row[l] = lam > 0.0 ? fwd_get(a, d, l) / lam : 0.0;
-        }
-        __syncthreads();
-        for (int q = threadIdx.x; q < d.L; q += blockDim.x) inv_put(a, d, q, [&](int m) { return row[m]; });
-        __syncthreads();
-        fft_smem(a, d);
-        for (int l = threadIdx.x; l < ny; l += blockDim.x) row[l] = inv_get(a, d, l);
-        __syncthreads();
-    }
+    const double2* tw = reinterpret_cast<const double2*>(smem);
+    double2* a = fft_rows(smem, d);
+    const int stride = spectral_row(d.L);
+    const int nx = dx.n, ny = d.n, k0 = blockIdx.x * sp.rows_b, R = min(sp.rows_b, nx - k0);
+    double* tile = reinterpret_cast<double*>(a + (size_t)sp.rows_b * stride);
+    load_twiddles(smem, d);
     for (int q = threadIdx.x; q < R * ny; q += blockDim.x) {
-        const int l = q / R, r = q % R, k = k0 + r;
-        if (k < nx) T2[(size_t)k + (size_t)l * nx] = tile[(size_t)r * ny + l];
+        const int r = q / ny, l = q - r * ny;
+        fwd_put(a + (size_t)r * stride, d, l, T[(size_t)(k0 + r) * ny + l]);
+    }
+    __syncthreads();
+    fft_smem(a, tw, d, R);
+    for (int q = threadIdx.x; q < R * ny; q += blockDim.x) {
+        const int r = q / ny, l = q - r * ny;
+        const double lam = ax * __ldg(dx.mu + k0 + r) + ay * __ldg(d.mu + l);
+        tile[q] = lam > 0.0 ? fwd_get(a + (size_t)r * stride, d, l) / lam : 0.0;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < R * d.L; q += blockDim.x) {
+        const int r = q / d.L, kk = q - r * d.L;
+        const double* row = tile + (size_t)r * ny;
+        inv_put(a + (size_t)r * stride, d, kk, [&](int m) { return row[m]; });
+    }
+    __syncthreads();
+    fft_smem(a, tw, d, R);
+    for (int q = threadIdx.x; q < R * ny; q += blockDim.x) {
+        const int r = q / ny, l = q - r * ny;
+        tile[q] = inv_get(a + (size_t)r * stride, d, l);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < R * ny; q += blockDim.x) {
+        const int l = q / R, r = q - l * R;
+        T2[(size_t)(k0 + r) + (size_t)l * nx] = tile[(size_t)r * ny + l];
     }
 }
 
-// C: inverse x transform of row j, x += e; the iteration count.
+// C: inverse x transform of rows j0 .. j0 + R - 1 (together), x += e; the iteration count.
 __global__ void __launch_bounds__(kSpecThreads) k_spec_c(Spectral sp, const double* __restrict__ T2, double* x,
                                                         CGScal* cg, int* iters_out) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (cg->done) return;
     const SpecDir& d = sp.dx;
-    double2* a = reinterpret_cast<double2*>(smem);
-    const int nx = d.n, j = blockIdx.x;
-    const double* row = T2 + (size_t)j * nx;
-    for (int q = threadIdx.x; q < d.L; q += blockDim.x) inv_put(a, d, q, [&](int m) { return row[m]; });
+    const double2* tw = reinterpret_cast<const double2*>(smem);
+    double2* a = fft_rows(smem, d);
+    const int stride = spectral_row(d.L);
+    const int nx = d.n, ny = sp.dy.n, j0 = blockIdx.x * sp.rows_c, R = min(sp.rows_c, ny - j0);
+    load_twiddles(smem, d);
+    for (int q = threadIdx.x; q < R * d.L; q += blockDim.x) {
+        const int r = q / d.L, kk = q - r * d.L;
+        const double* row = T2 + (size_t)(j0 + r) * nx;
+        inv_put(a + (size_t)r * stride, d, kk, [&](int m) { return __ldg(row + m); });
+    }
     __syncthreads();
-    fft_smem(a, d);
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) x[cidx(i, j, nx)] += inv_get(a, d, i);
+    fft_smem(a, tw, d, R);
+    for (int q = threadIdx.x; q < R * nx; q += blockDim.x) {
+        const int r = q / nx, i = q - r * nx;
+        x[cidx(i, j0 + r, nx)] += inv_get(a + (size_t)r * stride, d, i);
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         cg->iter += 1;
         if (iters_out) *iters_out = cg->iter;
@@ -241,8 +286,7 @@ cudaError_t spectral_configure(const Spectral& sp) {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_spec_b, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.smem_b);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_spec_c, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(16 * (size_t)sp.dx.L));
+        e = cudaFuncSetAttribute(k_spec_c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.smem_c);
     return e;
 }
 
@@ -251,11 +295,12 @@ void proj_spectral_iter(const Params& P, const Projection& pj, CGScal* cg, const
     const Spectral& sp = pj.sp;
     const MGLevel& L = pj.lev[0];
     const int ga = (L.ny + sp.rows_a - 1) / sp.rows_a, gb = (L.nx + sp.rows_b - 1) / sp.rows_b;
+    const int gc = (L.ny + sp.rows_c - 1) / sp.rows_c;
     // T = pj.z (modes, y contiguous), T2 = pj.w (modes, x contiguous)
     k_spec_a<<<ga, kSpecThreads, sp.smem_a, s>>>(sp, L, P.g.px, P.g.py, pj.b, pj.x, pj.z, ps, cg, rs, iters_out,
                                                   cond);
     k_spec_b<<<gb, kSpecThreads, sp.smem_b, s>>>(sp, L.ax, L.ay, pj.z, pj.w, cg);
-    k_spec_c<<<L.ny, kSpecThreads, 16 * (size_t)sp.dx.L, s>>>(sp, pj.w, pj.x, cg, iters_out);
+    k_spec_c<<<gc, kSpecThreads, sp.smem_c, s>>>(sp, pj.w, pj.x, cg, iters_out);
 }
 
 }  // namespace efsi
