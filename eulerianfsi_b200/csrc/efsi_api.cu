@@ -482,6 +482,10 @@ SpecDir spectral_dir(efsi_handle* h, int kind, int n) {
     d.L = (kind == SPEC_ND || kind == SPEC_DN) ? 2 * n : n;
     d.logL = 0;
     while ((1 << d.logL) < d.L) ++d.logL;
+    d.logn = 0;
+    while ((1 << d.logn) < n) ++d.logn;
+    d.inv_n = 1.0 / n;
+    d.inv_L = 1.0 / d.L;
     const long double pi = 3.141592653589793238462643383279502884L;
     std::vector<double2> w(std::max(1, d.L / 2)), mk(d.L);
     for (int t = 0; t < d.L / 2; ++t) {
@@ -530,15 +534,19 @@ void setup_spectral(efsi_handle* h, const HostLevel& L0, bool px, bool py) {
     auto smem = [](int L, int n, int R, bool tile) {
         return 16 * (size_t)(L / 2) + 16 * (size_t)R * spectral_row(L) + (tile ? 8 * (size_t)R * n : 0);
     };
-    auto rows = [&](int L, int n, bool tile) {
+    auto rows = [&](int L, int n, bool tile) {  // a power of two dividing the row count
         int R = 4;
-        while (R > 1 && smem(L, n, R, tile) > kBudget) --R;
+        while (R > 1 && smem(L, n, R, tile) > kBudget) R >>= 1;
         return smem(L, n, R, tile) <= kMax ? R : 0;
     };
-    sp.rows_a = rows(Lx, L0.nx, true);
-    sp.rows_b = rows(Ly, L0.ny, true);
-    sp.rows_c = rows(Lx, L0.nx, false);
+    sp.rows_a = std::min(rows(Lx, L0.nx, true), L0.ny);
+    sp.rows_b = std::min(rows(Ly, L0.ny, true), L0.nx);
+    sp.rows_c = std::min(rows(Lx, L0.nx, false), L0.ny);
     if (sp.rows_a < 1 || sp.rows_b < 1 || sp.rows_c < 1) return;
+    auto lg = [](int R) { int l = 0; while ((1 << l) < R) ++l; return l; };
+    sp.lg_a = lg(sp.rows_a);
+    sp.lg_b = lg(sp.rows_b);
+    sp.lg_c = lg(sp.rows_c);
     sp.smem_a = smem(Lx, L0.nx, sp.rows_a, true);
     sp.smem_b = smem(Ly, L0.ny, sp.rows_b, true);
     sp.smem_c = smem(Lx, L0.nx, sp.rows_c, false);

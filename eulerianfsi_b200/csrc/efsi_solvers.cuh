@@ -152,8 +152,9 @@ struct MGLevel {
 // diagonalised by a cosine, sine or Hartley transform computed with a complex FFT.
 enum SpecKind : int { SPEC_NN = 0, SPEC_DD = 1, SPEC_ND = 2, SPEC_DN = 3, SPEC_P = 4 };
 struct SpecDir {
-    int n;              // cells along the direction
+    int n, logn;        // cells along the direction (a power of two)
     int L, logL;        // complex FFT length (n, or 2n for the odd extension of ND / DN)
+    double inv_n, inv_L;  // 1 / n, 1 / L (exact)
     int kind;           // SpecKind
     const double2* w;   // exp(-2 pi i t / L), t < L / 2
     const double2* mk;  // exp(-i pi k / (2 L)), k < L (cosine-transform twiddles)
@@ -162,7 +163,8 @@ struct SpecDir {
 struct Spectral {
     bool on;
     SpecDir dx, dy;
-    int rows_a, rows_b, rows_c;  // rows (x passes) and modes (y pass) transformed per block
+    int rows_a, rows_b, rows_c;  // rows (x passes) and modes (y pass) transformed per block (powers of two)
+    int lg_a, lg_b, lg_c;        // their base-2 logarithms
     size_t smem_a, smem_b, smem_c;
 };
 // Padded complex elements of one FFT row of length L in shared memory (one spare per 32).

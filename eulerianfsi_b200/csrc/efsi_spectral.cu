@@ -54,11 +54,11 @@ __device__ __forceinline__ void load_twiddles(unsigned char* smem, const SpecDir
 // In-place radix-2 decimation-in-time FFT (forward sign) of R rows a[r * stride + pad(.)]
 // whose inputs are stored in bit-reversed order; ends with a barrier.
 __device__ void fft_smem(double2* a, const double2* tw, const SpecDir& d, int R) {
-    const int L = d.L, half = L / 2, stride = spectral_row(L);
+    const int L = d.L, half = L / 2, stride = spectral_row(L), lh = d.logL - 1;
     for (int s = 1; s <= d.logL; ++s) {
         const int h = 1 << (s - 1), ts = L >> s;
         for (int q = threadIdx.x; q < R * half; q += blockDim.x) {
-            const int r = q / half, qq = q - r * half;
+            const int r = q >> lh, qq = q & (half - 1);
             const int j = qq & (h - 1), i0 = ((qq >> (s - 1)) << s) + j;
             double2* row = a + (size_t)r * stride;
             const int p0 = pad(i0), p1 = pad(i0 + h);
@@ -130,13 +130,13 @@ __device__ __forceinline__ void inv_put(double2* a, const SpecDir& d, int k, con
 }
 // Inverse transform, output value at index i (0 <= i < n) of one row after the FFT.
 __device__ __forceinline__ double inv_get(const double2* a, const SpecDir& d, int i) {
-    if (d.kind == SPEC_P) {
+    if (d.kind == SPEC_P) {  // 1 / n and 1 / L are exact (powers of two)
         const double2 v = a[pad(i)];
-        return (v.x - v.y) / d.n;
+        return (v.x - v.y) * d.inv_n;
     }
     const int e = d.kind == SPEC_DN ? d.n - 1 - i : i;
     const int p = (e & 1) ? d.L - 1 - (e >> 1) : (e >> 1);
-    const double v = a[pad(p)].x / d.L;
+    const double v = a[pad(p)].x * d.inv_L;
     return (d.kind == SPEC_DD && (i & 1)) ? -v : v;
 }
 
@@ -173,13 +173,13 @@ __global__ void __launch_bounds__(kSpecThreads) k_spec_a(Spectral sp, MGLevel L0
     const double2* tw = reinterpret_cast<const double2*>(smem);
     double2* a = fft_rows(smem, d);
     const int stride = spectral_row(d.L);
-    const int nx = L0.nx, ny = L0.ny, j0 = blockIdx.x * sp.rows_a, R = min(sp.rows_a, ny - j0);
+    const int nx = L0.nx, ny = L0.ny, j0 = blockIdx.x * sp.rows_a, R = sp.rows_a;  // R divides ny
     double* tile = reinterpret_cast<double*>(a + (size_t)sp.rows_a * stride);
     const double bmean = ps->v[10];
     load_twiddles(smem, d);
     double acc[1] = {0.0};
     for (int q = threadIdx.x; q < R * nx; q += blockDim.x) {
-        const int r = q / nx, i = q - r * nx, j = j0 + r;
+        const int r = q >> d.logn, i = q & (nx - 1), j = j0 + r;
         const double v = (b[cidx(i, j, nx)] - bmean) - apply_K(L0, px, py, x, i, j);
         acc[0] += v * v;
         fwd_put(a + (size_t)r * stride, d, i, v);
@@ -187,12 +187,12 @@ __global__ void __launch_bounds__(kSpecThreads) k_spec_a(Spectral sp, MGLevel L0
     __syncthreads();
     fft_smem(a, tw, d, R);
     for (int q = threadIdx.x; q < R * nx; q += blockDim.x) {
-        const int r = q / nx, k = q - r * nx;
+        const int r = q >> d.logn, k = q & (nx - 1);
         tile[q] = fwd_get(a + (size_t)r * stride, d, k);
     }
     __syncthreads();
     for (int q = threadIdx.x; q < R * nx; q += blockDim.x) {
-        const int k = q / R, r = q - k * R;
+        const int k = q >> sp.lg_a, r = q & (R - 1);
         T[(size_t)(j0 + r) + (size_t)k * ny] = tile[r * nx + k];
     }
     double tot[1];
@@ -217,35 +217,35 @@ __global__ void __launch_bounds__(kSpecThreads) k_spec_b(Spectral sp, double ax,
     const double2* tw = reinterpret_cast<const double2*>(smem);
     double2* a = fft_rows(smem, d);
     const int stride = spectral_row(d.L);
-    const int nx = dx.n, ny = d.n, k0 = blockIdx.x * sp.rows_b, R = min(sp.rows_b, nx - k0);
+    const int nx = dx.n, ny = d.n, k0 = blockIdx.x * sp.rows_b, R = sp.rows_b;  // R divides nx
     double* tile = reinterpret_cast<double*>(a + (size_t)sp.rows_b * stride);
     load_twiddles(smem, d);
     for (int q = threadIdx.x; q < R * ny; q += blockDim.x) {
-        const int r = q / ny, l = q - r * ny;
+        const int r = q >> d.logn, l = q & (ny - 1);
         fwd_put(a + (size_t)r * stride, d, l, T[(size_t)(k0 + r) * ny + l]);
     }
     __syncthreads();
     fft_smem(a, tw, d, R);
     for (int q = threadIdx.x; q < R * ny; q += blockDim.x) {
-        const int r = q / ny, l = q - r * ny;
+        const int r = q >> d.logn, l = q & (ny - 1);
         const double lam = ax * __ldg(dx.mu + k0 + r) + ay * __ldg(d.mu + l);
         tile[q] = lam > 0.0 ? fwd_get(a + (size_t)r * stride, d, l) / lam : 0.0;
     }
     __syncthreads();
     for (int q = threadIdx.x; q < R * d.L; q += blockDim.x) {
-        const int r = q / d.L, kk = q - r * d.L;
+        const int r = q >> d.logL, kk = q & (d.L - 1);
         const double* row = tile + (size_t)r * ny;
         inv_put(a + (size_t)r * stride, d, kk, [&](int m) { return row[m]; });
     }
     __syncthreads();
     fft_smem(a, tw, d, R);
     for (int q = threadIdx.x; q < R * ny; q += blockDim.x) {
-        const int r = q / ny, l = q - r * ny;
+        const int r = q >> d.logn, l = q & (ny - 1);
         tile[q] = inv_get(a + (size_t)r * stride, d, l);
     }
     __syncthreads();
     for (int q = threadIdx.x; q < R * ny; q += blockDim.x) {
-        const int l = q / R, r = q - l * R;
+        const int l = q >> sp.lg_b, r = q & (R - 1);
         T2[(size_t)(k0 + r) + (size_t)l * nx] = tile[(size_t)r * ny + l];
     }
 }
@@ -259,17 +259,17 @@ __global__ void __launch_bounds__(kSpecThreads) k_spec_c(Spectral sp, const doub
     const double2* tw = reinterpret_cast<const double2*>(smem);
     double2* a = fft_rows(smem, d);
     const int stride = spectral_row(d.L);
-    const int nx = d.n, ny = sp.dy.n, j0 = blockIdx.x * sp.rows_c, R = min(sp.rows_c, ny - j0);
+    const int nx = d.n, j0 = blockIdx.x * sp.rows_c, R = sp.rows_c;  // R divides ny
     load_twiddles(smem, d);
     for (int q = threadIdx.x; q < R * d.L; q += blockDim.x) {
-        const int r = q / d.L, kk = q - r * d.L;
+        const int r = q >> d.logL, kk = q & (d.L - 1);
         const double* row = T2 + (size_t)(j0 + r) * nx;
         inv_put(a + (size_t)r * stride, d, kk, [&](int m) { return __ldg(row + m); });
     }
     __syncthreads();
     fft_smem(a, tw, d, R);
     for (int q = threadIdx.x; q < R * nx; q += blockDim.x) {
-        const int r = q / nx, i = q - r * nx;
+        const int r = q >> d.logn, i = q & (nx - 1);
         x[cidx(i, j0 + r, nx)] += inv_get(a + (size_t)r * stride, d, i);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
