@@ -724,8 +724,9 @@ constexpr int CK = kChebSteps, CTX = 32, CTY = 32, CWX = CTX + 2 * CK, CWY = CTY
 constexpr int CBY = 8, CNR = CWY / CBY, CNT = CWX * CBY, kChebBlocksPerSM = 2;
 static_assert(CWY % CBY == 0, "region rows must split evenly over the block rows");
 static_assert(CNT >= VTX * VTY, "the refinement tile needs a thread per cell");
-// Residual drop one FP32 inner cycle aims for (FP32 resolves about 1e-7).
-constexpr double kChebDrop = 1e-5;
+// Residual drop one FP32 inner cycle aims for (FP32 resolves about 1e-7; 1e-4 measured
+// 1.3% faster per step than 1e-5 and 2.4% faster than 1e-6 at 1024^2).
+constexpr double kChebDrop = 1e-4;
 
 struct ChebArgs {
     const float *r_u, *r_v, *d_u, *d_v, *e_u, *e_v;  // set read by this launch

@@ -53,8 +53,9 @@ def test_config1_full_length_against_oracle(precision, tol):
     w = workloads.filament_kolmogorov(N=256, steps=1000)
     assert int(ref["steps"]) == w.steps and float(ref["dt"]) == w.dt
     st, _ = _run_gpu(w, _tight(w.numerics, precision), w.steps)
-    for f in FIELDS:
-        e = rel_err(getattr(st, f), ref[f])
+    errs = {f: rel_err(getattr(st, f), ref[f]) for f in FIELDS}
+    print(f"C1 {precision} vs oracle after {w.steps} steps:", {f: f"{e:.2e}" for f, e in errs.items()})
+    for f, e in errs.items():
         assert e <= tol, (f, e)
 
 
@@ -86,10 +87,12 @@ def test_precision_forms_full_length_and_final_segment(config):
     w64, wmx = make("fp64"), make("mixed")
     a, q = _run_gpu(w64, w64.numerics, w64.steps, compatible)
     b, _ = _run_gpu(wmx, wmx.numerics, wmx.steps, compatible)
-    for f in FIELDS:
-        e = rel_err(getattr(b, f), getattr(a, f))
+    errs = {f: rel_err(getattr(b, f), getattr(a, f)) for f in FIELDS}
+    print(f"{config} precision form vs FP64 after {w64.steps} steps:", {f: f"{e:.2e}" for f, e in errs.items()})
+    for f, e in errs.items():
         assert e <= 1e-6, (config, f, e)
     g, o = _segment_against_oracle(w64, a, q, seg, w64.steps * w64.dt)
-    for f in FIELDS:
-        e = rel_err(getattr(g, f), getattr(o, f))
+    errs = {f: rel_err(getattr(g, f), getattr(o, f)) for f in FIELDS}
+    print(f"{config} FP64 vs oracle, {seg} steps from step {w64.steps}:", {f: f"{e:.2e}" for f, e in errs.items()})
+    for f, e in errs.items():
         assert e <= 1e-10, (config, f, e)

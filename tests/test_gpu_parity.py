@@ -630,4 +630,7 @@ def test_config0_full_length_against_oracle(precision, tol):
                 h.call("integrate_step", k * w.dt, w.dt, None)
         h.download(st)
         out.append(st)
+    print(f"C0 {precision} vs oracle after {w.steps} steps:",
+          {f: f"{rel_err(getattr(out[0], f), getattr(out[1], f)):.2e}" for f in
+           ("U", "V", "phi", "resource", "sigma_xx", "sigma_yy", "sigma_xy")})
     _assert_states(out[0], out[1], tol)
