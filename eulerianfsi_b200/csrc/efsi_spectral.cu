@@ -51,22 +51,50 @@ __device__ __forceinline__ void load_twiddles(unsigned char* smem, const SpecDir
     for (int t = threadIdx.x; t < d.L / 2; t += blockDim.x) tw[t] = __ldg(d.w + t);
 }
 
-// In-place radix-2 decimation-in-time FFT (forward sign) of R rows a[r * stride + pad(.)]
-// whose inputs are stored in bit-reversed order; ends with a barrier.
-__device__ void fft_smem(double2* a, const double2* tw, const SpecDir& d, int R) {
-    const int L = d.L, half = L / 2, stride = spectral_row(L), lh = d.logL - 1;
-    for (int s = 1; s <= d.logL; ++s) {
-        const int h = 1 << (s - 1), ts = L >> s;
-        for (int q = threadIdx.x; q < R * half; q += blockDim.x) {
-            const int r = q >> lh, qq = q & (half - 1);
-            const int j = qq & (h - 1), i0 = ((qq >> (s - 1)) << s) + j;
-            double2* row = a + (size_t)r * stride;
-            const int p0 = pad(i0), p1 = pad(i0 + h);
-            const double2 t = cmul(tw[j * ts], row[p1]), u = row[p0];
-            row[p0] = make_double2(u.x + t.x, u.y + t.y);
-            row[p1] = make_double2(u.x - t.x, u.y - t.y);
+// W consecutive radix-2 decimation-in-time stages s0 + 1 .. s0 + W (stage s pairs
+// elements 2^(s-1) apart, twiddle exp(-2 pi i j / 2^s) for the pair's offset j within its
+// half-block) done in registers on groups of 2^W elements {b + j + m 2^s0}: one shared-
+// memory read and write of each element and one barrier per W stages instead of per
+// stage.  With the padded layout a warp's 16-byte accesses of one m fall on distinct
+// bank groups for every distance (consecutive j, or contiguous runs of 8 for s0 = 0).
+template <int W>
+__device__ __forceinline__ void fft_pass(double2* a, const double2* tw, int L, int logL, int stride, int s0, int R) {
+    constexpr int M = 1 << W;
+    const int h = 1 << s0, lg = logL - W, G = L >> W;  // G groups per row
+    for (int q = threadIdx.x; q < R * G; q += blockDim.x) {
+        const int r = q >> lg, g = q & (G - 1);
+        const int j = g & (h - 1), b = (g >> s0) << (s0 + W);
+        double2* row = a + (size_t)r * stride;
+        double2 v[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) v[m] = row[pad(b + j + m * h)];
+#pragma unroll
+        for (int t = 0; t < W; ++t) {
+            const int hs = 1 << t, ts = L >> (s0 + t + 1);
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                if (m & hs) continue;  // m is the lower element of the pair (m, m + hs)
+                const double2 x = cmul(tw[(j + (m & (hs - 1)) * h) * ts], v[m + hs]), u = v[m];
+                v[m] = make_double2(u.x + x.x, u.y + x.y);
+                v[m + hs] = make_double2(u.x - x.x, u.y - x.y);
+            }
         }
-        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < M; ++m) row[pad(b + j + m * h)] = v[m];
+    }
+    __syncthreads();
+}
+
+// In-place FFT (forward sign) of R rows a[r * stride + pad(.)] whose inputs are stored in
+// bit-reversed order, as radix-8 register passes (the last pass radix-4 or radix-2 when
+// log2 L is not a multiple of 3); ends with a barrier.
+__device__ void fft_smem(double2* a, const double2* tw, const SpecDir& d, int R) {
+    const int L = d.L, stride = spectral_row(L);
+    for (int s0 = 0; s0 < d.logL;) {
+        const int w = d.logL - s0;
+        if (w >= 3) { fft_pass<3>(a, tw, L, d.logL, stride, s0, R); s0 += 3; }
+        else if (w == 2) { fft_pass<2>(a, tw, L, d.logL, stride, s0, R); s0 += 2; }
+        else { fft_pass<1>(a, tw, L, d.logL, stride, s0, R); s0 += 1; }
     }
 }
 
