@@ -777,14 +777,15 @@ void proj_solve(efsi_handle* h, int stage_slot, double reltol, const double* q0)
     const double N = (double)h->nc;
     if (h->pj.sp.on) {  // direct fast-diagonalisation solve inside a Richardson iteration
         solve(
-            h, KIND_PROJ, stage_slot, &d->cg_proj, P.nu.projection_maxiter, 3, 1,
+            h, KIND_PROJ, stage_slot, &d->cg_proj, P.nu.projection_maxiter, 4, 1,
             [&](cudaStream_t s, int* io, cudaGraphConditionalHandle ch) {
                 proj_spectral_init(P, h->pj, reltol, P.nu.projection_maxiter, q0, &d->cg_proj, &d->ps, h->slot[1],
                                    &d->st, io, ch, s);
                 h->launches += 1;
             },
             [&](cudaStream_t s, int* io, cudaGraphConditionalHandle ch) {
-                // residual + x transform (2 x 8 N B), y pass (2 x 8 N), x pass + update (3 x 8 N)
+                // x transform (2 x 8 N B), y pass (2 x 8 N), x pass + update (3 x 8 N),
+                // residual (3 x 8 N)
                 site(h, EFSI_SITE_SPECTRAL, 8.0 * N * 9.0,
                      [&] { proj_spectral_iter(P, h->pj, &d->cg_proj, &d->ps, h->slot[4], io, ch, s); });
             });

@@ -19,12 +19,14 @@
 // of a Richardson iteration x += K^-1 (b - K x) judged by the FP64 residual, so the
 // projection's relative tolerance keeps its meaning; one iteration reaches about 1e-13.
 //
-// Data flow of one iteration (three launches, the arrays stay L2-resident at 1024^2):
-//   A  rows j: r = (b - mean) - K x (FP64, |r|^2 decides convergence), x transform of r,
-//      modes written transposed (T[j + k Ny]);
+// Data flow of one iteration (four launches, the arrays stay L2-resident at 1024^2); the
+// solve's init has stored r = (b - mean) - K x0 and decided on it:
+//   A  rows j: x transform of r, modes written transposed (T[j + k Ny]);
 //   B  modes k: y transform, division by the eigenvalue, inverse y transform, written
 //      transposed back (T2[k + j Nx]);
-//   C  rows j: inverse x transform, x += e.
+//   C  rows j: inverse x transform, x += e;
+//   R  cells: r = (b - mean) - K x (FP64, stored), |r|^2 decides convergence.
+// A converged solve therefore ends after its R, with no transform spent on the test.
 #include "efsi_solvers.cuh"
 
 namespace efsi {
@@ -188,53 +190,33 @@ __device__ __forceinline__ double apply_K(const MGLevel& L, int px, int py, cons
     return d * x[k] - off;
 }
 
-// A: residual and x transform of rows j0 .. j0 + R - 1 (transformed together); the
-// modes go to the tile and from there transposed to T; convergence decision.
-__global__ void __launch_bounds__(kSpecThreads) k_spec_a(Spectral sp, MGLevel L0, int px, int py,
-                                                        const double* __restrict__ b, const double* __restrict__ x,
-                                                        double* __restrict__ T, const ProjScal* ps, CGScal* cg,
-                                                        RedSlot rs, int* iters_out, cudaGraphConditionalHandle cond) {
+// A: x transform of the residual rows j0 .. j0 + R - 1 (transformed together); the
+// modes go to the tile and from there transposed to T.
+__global__ void __launch_bounds__(kSpecThreads) k_spec_a(Spectral sp, int nx, int ny, const double* __restrict__ r,
+                                                        double* __restrict__ T, const CGScal* cg) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ double sh[32];
     if (cg->done) return;
     const SpecDir& d = sp.dx;
     const double2* tw = reinterpret_cast<const double2*>(smem);
     double2* a = fft_rows(smem, d);
     const int stride = spectral_row(d.L);
-    const int nx = L0.nx, ny = L0.ny, j0 = blockIdx.x * sp.rows_a, R = sp.rows_a;  // R divides ny
+    const int j0 = blockIdx.x * sp.rows_a, R = sp.rows_a;  // R divides ny
     double* tile = reinterpret_cast<double*>(a + (size_t)sp.rows_a * stride);
-    const double bmean = ps->v[10];
     load_twiddles(smem, d);
-    double acc[1] = {0.0};
     for (int q = threadIdx.x; q < R * nx; q += blockDim.x) {
-        const int r = q >> d.logn, i = q & (nx - 1), j = j0 + r;
-        const double v = (b[cidx(i, j, nx)] - bmean) - apply_K(L0, px, py, x, i, j);
-        acc[0] += v * v;
-        fwd_put(a + (size_t)r * stride, d, i, v);
+        const int rr = q >> d.logn, i = q & (nx - 1);
+        fwd_put(a + (size_t)rr * stride, d, i, __ldg(r + cidx(i, j0 + rr, nx)));
     }
     __syncthreads();
     fft_smem(a, tw, d, R);
     for (int q = threadIdx.x; q < R * nx; q += blockDim.x) {
-        const int r = q >> d.logn, k = q & (nx - 1);
-        tile[q] = fwd_get(a + (size_t)r * stride, d, k);
+        const int rr = q >> d.logn, k = q & (nx - 1);
+        tile[q] = fwd_get(a + (size_t)rr * stride, d, k);
     }
     __syncthreads();
     for (int q = threadIdx.x; q < R * nx; q += blockDim.x) {
-        const int k = q >> sp.lg_a, r = q & (R - 1);
-        T[(size_t)(j0 + r) + (size_t)k * ny] = tile[r * nx + k];
-    }
-    double tot[1];
-    if (grid_reduce<1>(acc, rs, tot, sh) && threadIdx.x == 0) {
-        // With the exact inverse a pass leaves only the rounding of K x and of the
-        // transforms (about eps |K| |x|); a pass that does not halve the residual is at
-        // that floor, which no further pass lowers: accepted as converged (the
-        // projection's true-residual test still judges it against its own tolerance).
-        const bool stalled = cg->iter > 0 && tot[0] > 0.25 * cg->rr;
-        cg->rr = tot[0];
-        if (tot[0] <= cg->tol2 || (stalled && isfinite(tot[0]))) { cg->conv = 1; cg->done = 1; }
-        else if (cg->iter >= cg->maxiter || !isfinite(tot[0])) cg->done = 1;
-        if (iters_out) *iters_out = cg->iter;
-        set_loop(cond, !cg->done);
+        const int k = q >> sp.lg_a, rr = q & (R - 1);
+        T[(size_t)(j0 + rr) + (size_t)k * ny] = tile[rr * nx + k];
     }
 }
 
@@ -311,6 +293,40 @@ __global__ void __launch_bounds__(kSpecThreads) k_spec_c(Spectral sp, const doub
     }
 }
 
+// R: after a pass, r = (b - mean) - K x (stored for the next pass's transform) and its
+// squared norm over the grid; the convergence decision of the Richardson iteration.
+__global__ void __launch_bounds__(kSpecThreads) k_spec_r(MGLevel L0, int logn, int px, int py,
+                                                        const double* __restrict__ b, const double* __restrict__ x,
+                                                        double* __restrict__ r, const ProjScal* ps, CGScal* cg,
+                                                        RedSlot rs, int* iters_out, cudaGraphConditionalHandle cond) {
+    __shared__ double sh[32];
+    if (cg->done) return;
+    const int nx = L0.nx;
+    const size_t nc = (size_t)nx * L0.ny;
+    const double bmean = ps->v[10];
+    double acc[1] = {0.0};
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nc; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q & (size_t)(nx - 1)), j = (int)(q >> logn);
+        const size_t k = cidx(i, j, nx);
+        const double v = (b[k] - bmean) - apply_K(L0, px, py, x, i, j);
+        r[k] = v;
+        acc[0] += v * v;
+    }
+    double tot[1];
+    if (grid_reduce<1>(acc, rs, tot, sh) && threadIdx.x == 0) {
+        // With the exact inverse a pass leaves only the rounding of K x and of the
+        // transforms (about eps |K| |x|); a pass that does not halve the residual is at
+        // that floor, which no further pass lowers: accepted as converged (the
+        // projection's true-residual test still judges it against its own tolerance).
+        const bool stalled = tot[0] > 0.25 * cg->rr;
+        cg->rr = tot[0];
+        if (tot[0] <= cg->tol2 || (stalled && isfinite(tot[0]))) { cg->conv = 1; cg->done = 1; }
+        else if (cg->iter >= cg->maxiter || !isfinite(tot[0])) cg->done = 1;
+        if (iters_out) *iters_out = cg->iter;
+        set_loop(cond, !cg->done);
+    }
+}
+
 }  // namespace
 
 cudaError_t spectral_configure(const Spectral& sp) {
@@ -329,11 +345,15 @@ void proj_spectral_iter(const Params& P, const Projection& pj, CGScal* cg, const
     const MGLevel& L = pj.lev[0];
     const int ga = (L.ny + sp.rows_a - 1) / sp.rows_a, gb = (L.nx + sp.rows_b - 1) / sp.rows_b;
     const int gc = (L.ny + sp.rows_c - 1) / sp.rows_c;
+    // r = pj.r[0] (the residual, from the solve's init or the previous pass's R),
     // T = pj.z (modes, y contiguous), T2 = pj.w (modes, x contiguous)
-    k_spec_a<<<ga, kSpecThreads, sp.smem_a, s>>>(sp, L, P.g.px, P.g.py, pj.b, pj.x, pj.z, ps, cg, rs, iters_out,
-                                                  cond);
+    k_spec_a<<<ga, kSpecThreads, sp.smem_a, s>>>(sp, L.nx, L.ny, pj.r[0], pj.z, cg);
     k_spec_b<<<gb, kSpecThreads, sp.smem_b, s>>>(sp, L.ax, L.ay, pj.z, pj.w, cg);
     k_spec_c<<<gc, kSpecThreads, sp.smem_c, s>>>(sp, pj.w, pj.x, cg, iters_out);
+    const size_t nc = (size_t)L.nx * L.ny;
+    const int gr = (int)std::min<size_t>((nc + kSpecThreads - 1) / kSpecThreads, (size_t)std::max(P.nsm, 1) * 8);
+    k_spec_r<<<gr, kSpecThreads, 0, s>>>(L, sp.dx.logn, P.g.px, P.g.py, pj.b, pj.x, pj.r[0], ps, cg, rs, iters_out,
+                                         cond);
 }
 
 }  // namespace efsi
