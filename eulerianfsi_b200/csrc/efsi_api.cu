@@ -528,11 +528,11 @@ void setup_spectral(efsi_handle* h, const HostLevel& L0, bool px, bool py) {
     if (kx < 0 || ky < 0) return;
     const int Lx = (kx == SPEC_ND || kx == SPEC_DN) ? 2 * L0.nx : L0.nx;
     const int Ly = (ky == SPEC_ND || ky == SPEC_DN) ? 2 * L0.ny : L0.ny;
-    // per block: L/2 twiddles, R padded FFT rows and (A, B) an R x n tile of modes; at
+    // per block: L/2 twiddles, R padded FFT rows and (A, B) an R x (n + 8) tile of modes; at
     // most four rows, and at most ~112 KB so that two blocks share an SM
     constexpr size_t kBudget = 112 * 1024, kMax = 220 * 1024;
     auto smem = [](int L, int n, int R, bool tile) {
-        return 16 * (size_t)(L / 2) + 16 * (size_t)R * spectral_row(L) + (tile ? 8 * (size_t)R * n : 0);
+        return 16 * (size_t)(L / 2) + 16 * (size_t)R * spectral_row(L) + (tile ? 8 * (size_t)R * (n + 8) : 0);
     };
     auto rows = [&](int L, int n, bool tile) {  // a power of two dividing the row count
         int R = 4;

@@ -33,7 +33,7 @@ namespace efsi {
 
 namespace {
 
-constexpr int kSpecThreads = 256;
+constexpr int kSpecThreads = 512;  // with at most 64 registers: two blocks (the shared-memory limit) fill an SM
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -43,14 +43,26 @@ __device__ __forceinline__ int brev(int i, int logL) { return (int)(__brev((unsi
 // bit-reversed scatters and the butterflies of a warp spread over the banks).
 __device__ __forceinline__ int pad(int i) { return i + (i >> 5); }
 
-// Shared-memory layout of one block: the L/2 twiddles, then R FFT rows of spectral_row(L)
-// padded elements (R rows are transformed at once, with the same barriers as one).
+// Slot of twiddle t in shared memory: the low three bits are XORed with a fold of the
+// higher bits, so that the power-of-two strides of the butterfly passes (t = j ts over
+// consecutive j) spread over the eight 16-byte bank groups; a permutation of [0, L/2).
+__device__ __forceinline__ int twz(int t) {
+    const int x = t >> 3;
+    return t ^ ((x ^ (x >> 3) ^ (x >> 6) ^ (x >> 9)) & 7);
+}
+// Row stride (doubles) of the transposed-mode tiles: rows padded by 8 doubles, so that
+// the column-wise reads of four rows fall on different banks.
+__device__ __forceinline__ int tile_row(int n) { return n + 8; }
+
+// Shared-memory layout of one block: the L/2 twiddles (slots twz(t)), then R FFT rows of
+// spectral_row(L) padded elements (R rows are transformed at once, with the same
+// barriers as one).
 __device__ __forceinline__ double2* fft_rows(unsigned char* smem, const SpecDir& d) {
     return reinterpret_cast<double2*>(smem) + d.L / 2;
 }
 __device__ __forceinline__ void load_twiddles(unsigned char* smem, const SpecDir& d) {
     double2* tw = reinterpret_cast<double2*>(smem);
-    for (int t = threadIdx.x; t < d.L / 2; t += blockDim.x) tw[t] = __ldg(d.w + t);
+    for (int t = threadIdx.x; t < d.L / 2; t += blockDim.x) tw[twz(t)] = __ldg(d.w + t);
 }
 
 // W consecutive radix-2 decimation-in-time stages s0 + 1 .. s0 + W (stage s pairs
@@ -76,7 +88,7 @@ __device__ __forceinline__ void fft_pass(double2* a, const double2* tw, int L, i
 #pragma unroll
             for (int m = 0; m < M; ++m) {
                 if (m & hs) continue;  // m is the lower element of the pair (m, m + hs)
-                const double2 x = cmul(tw[(j + (m & (hs - 1)) * h) * ts], v[m + hs]), u = v[m];
+                const double2 x = cmul(tw[twz((j + (m & (hs - 1)) * h) * ts)], v[m + hs]), u = v[m];
                 v[m] = make_double2(u.x + x.x, u.y + x.y);
                 v[m + hs] = make_double2(u.x - x.x, u.y - x.y);
             }
@@ -192,7 +204,7 @@ __device__ __forceinline__ double apply_K(const MGLevel& L, int px, int py, cons
 
 // A: x transform of the residual rows j0 .. j0 + R - 1 (transformed together); the
 // modes go to the tile and from there transposed to T.
-__global__ void __launch_bounds__(kSpecThreads) k_spec_a(Spectral sp, int nx, int ny, const double* __restrict__ r,
+__global__ void __launch_bounds__(kSpecThreads, 2) k_spec_a(Spectral sp, int nx, int ny, const double* __restrict__ r,
                                                         double* __restrict__ T, const CGScal* cg) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (cg->done) return;
@@ -211,18 +223,18 @@ __global__ void __launch_bounds__(kSpecThreads) k_spec_a(Spectral sp, int nx, in
     fft_smem(a, tw, d, R);
     for (int q = threadIdx.x; q < R * nx; q += blockDim.x) {
         const int rr = q >> d.logn, k = q & (nx - 1);
-        tile[q] = fwd_get(a + (size_t)rr * stride, d, k);
+        tile[rr * tile_row(nx) + k] = fwd_get(a + (size_t)rr * stride, d, k);
     }
     __syncthreads();
     for (int q = threadIdx.x; q < R * nx; q += blockDim.x) {
         const int k = q >> sp.lg_a, rr = q & (R - 1);
-        T[(size_t)(j0 + rr) + (size_t)k * ny] = tile[rr * nx + k];
+        T[(size_t)(j0 + rr) + (size_t)k * ny] = tile[rr * tile_row(nx) + k];
     }
 }
 
 // B: y transform of modes k0 .. k0 + R - 1 (together), division by the eigenvalue,
 // inverse y transform, written transposed to T2.
-__global__ void __launch_bounds__(kSpecThreads) k_spec_b(Spectral sp, double ax, double ay,
+__global__ void __launch_bounds__(kSpecThreads, 2) k_spec_b(Spectral sp, double ax, double ay,
                                                         const double* __restrict__ T, double* __restrict__ T2,
                                                         const CGScal* cg) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -244,29 +256,29 @@ __global__ void __launch_bounds__(kSpecThreads) k_spec_b(Spectral sp, double ax,
     for (int q = threadIdx.x; q < R * ny; q += blockDim.x) {
         const int r = q >> d.logn, l = q & (ny - 1);
         const double lam = ax * __ldg(dx.mu + k0 + r) + ay * __ldg(d.mu + l);
-        tile[q] = lam > 0.0 ? fwd_get(a + (size_t)r * stride, d, l) / lam : 0.0;
+        tile[r * tile_row(ny) + l] = lam > 0.0 ? fwd_get(a + (size_t)r * stride, d, l) / lam : 0.0;
     }
     __syncthreads();
     for (int q = threadIdx.x; q < R * d.L; q += blockDim.x) {
         const int r = q >> d.logL, kk = q & (d.L - 1);
-        const double* row = tile + (size_t)r * ny;
+        const double* row = tile + (size_t)r * tile_row(ny);
         inv_put(a + (size_t)r * stride, d, kk, [&](int m) { return row[m]; });
     }
     __syncthreads();
     fft_smem(a, tw, d, R);
     for (int q = threadIdx.x; q < R * ny; q += blockDim.x) {
         const int r = q >> d.logn, l = q & (ny - 1);
-        tile[q] = inv_get(a + (size_t)r * stride, d, l);
+        tile[r * tile_row(ny) + l] = inv_get(a + (size_t)r * stride, d, l);
     }
     __syncthreads();
     for (int q = threadIdx.x; q < R * ny; q += blockDim.x) {
         const int l = q >> sp.lg_b, r = q & (R - 1);
-        T2[(size_t)(k0 + r) + (size_t)l * nx] = tile[(size_t)r * ny + l];
+        T2[(size_t)(k0 + r) + (size_t)l * nx] = tile[r * tile_row(ny) + l];
     }
 }
 
 // C: inverse x transform of rows j0 .. j0 + R - 1 (together), x += e; the iteration count.
-__global__ void __launch_bounds__(kSpecThreads) k_spec_c(Spectral sp, const double* __restrict__ T2, double* x,
+__global__ void __launch_bounds__(kSpecThreads, 2) k_spec_c(Spectral sp, const double* __restrict__ T2, double* x,
                                                         CGScal* cg, int* iters_out) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (cg->done) return;
@@ -295,7 +307,7 @@ __global__ void __launch_bounds__(kSpecThreads) k_spec_c(Spectral sp, const doub
 
 // R: after a pass, r = (b - mean) - K x (stored for the next pass's transform) and its
 // squared norm over the grid; the convergence decision of the Richardson iteration.
-__global__ void __launch_bounds__(kSpecThreads) k_spec_r(MGLevel L0, int logn, int px, int py,
+__global__ void __launch_bounds__(kSpecThreads, 2) k_spec_r(MGLevel L0, int logn, int px, int py,
                                                         const double* __restrict__ b, const double* __restrict__ x,
                                                         double* __restrict__ r, const ProjScal* ps, CGScal* cg,
                                                         RedSlot rs, int* iters_out, cudaGraphConditionalHandle cond) {
