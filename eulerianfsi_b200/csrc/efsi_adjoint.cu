@@ -175,6 +175,15 @@ __device__ __forceinline__ Dn<K> dhypot(const Dn<K>& a, const Dn<K>& b) {
     for (int k = 0; k < K; ++k) r.d[k] = ia * a.d[k] + ib * b.d[k];
     return r;
 }
+template <int K>
+__device__ __forceinline__ Dn<K> dlog1p(const Dn<K>& a) {
+    Dn<K> r;
+    r.v = log1p(a.v);
+    const double g = 1.0 / (1.0 + a.v);
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = g * a.d[k];
+    return r;
+}
 // sech^2(x) = 1 - tanh^2(x) from e = exp(-2|x|): 4e / (1 + e)^2 keeps its full relative
 // accuracy where it is tiny (|x| large), unlike the difference 1 - tanh^2, whose rounding
 // error there is larger than the value itself.
@@ -758,7 +767,17 @@ __global__ void k_adj_acdi_psi(Params P, const double* __restrict__ phi, AdjScra
 // =====================================================================================
 // Structure tensor (StructureTensor.jl:377-551; k_structure)
 // =====================================================================================
-// sigma log sigma of an SPD 2x2 tensor (a, d, b) (StructureTensor.jl:482-515).
+// sigma log sigma of an SPD 2x2 tensor (a, d, b) (StructureTensor.jl:482-515):
+// alpha sigma + beta I with eigenvalues m +- r, alpha = (g(m + r) - g(m - r)) / 2r and
+// beta = (l+ g(m - r) - l- g(m + r)) / 2r for g(l) = l log l.  The forward's divided
+// difference is exact in value up to rounding, but its derivative cancels two terms of
+// size |dm| / r, which leaves an error of about eps m / r where the eigenvalues nearly
+// coincide (1e-12 m < r << m: nearly isotropic tensors next to the reset region).  The
+// reverse sweep therefore differentiates the same functions written in u = (r / m)^2,
+// which is smooth in (a, d, b):
+//   alpha = log m + F(u) + log(1 - u) / 2,  beta = -m (1 - u) F(u),
+//   F(u) = atanh(sqrt u) / sqrt u = sum_k u^k / (2k + 1)  (the series below u = 1e-4).
+// r <= 1e-12 scale keeps the forward's isotropic branch.
 template <int K>
 __device__ bool sigma_log_product_d(const Dn<K>& a, const Dn<K>& d, const Dn<K>& b, Dn<K>& oxx, Dn<K>& oyy,
                                     Dn<K>& oxy) {
@@ -766,16 +785,22 @@ __device__ bool sigma_log_product_d(const Dn<K>& a, const Dn<K>& d, const Dn<K>&
     Dn<K> r = dhypot(del, b);
     Dn<K> lhi = m + r, llo = m - r;
     if (!(isfinite(llo.v) && isfinite(lhi.v) && llo.v > 0.0)) return false;
-    Dn<K> ghi = lhi * dlog(lhi), glo = llo * dlog(llo);
     const double scale = fmax(1.0, fabs(m.v));
     Dn<K> alpha, beta;
     if (r.v <= 1.0e-12 * scale) {
         alpha = dlog(m) + 1.0;
         beta = -m;
     } else {
-        Dn<K> den = lhi - llo;
-        alpha = (ghi - glo) / den;
-        beta = (lhi * glo - llo * ghi) / den;
+        Dn<K> u = (del * del + b * b) / (m * m);
+        Dn<K> F;
+        if (u.v < 1.0e-4) {
+            F = 1.0 + u * (1.0 / 3.0 + u * (1.0 / 5.0 + u * (1.0 / 7.0 + u * (1.0 / 9.0 + u * (1.0 / 11.0)))));
+        } else {
+            Dn<K> t = dsqrt(u);
+            F = 0.5 * (dlog1p(t) - dlog1p(-t)) / t;
+        }
+        alpha = dlog(m) + F + 0.5 * dlog1p(-u);
+        beta = -(m * (1.0 - u) * F);
     }
     oxx = alpha * a + beta;
     oyy = alpha * d + beta;
