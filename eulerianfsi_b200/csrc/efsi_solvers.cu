@@ -723,7 +723,6 @@ constexpr int CK = kChebSteps, CTX = 32, CTY = 32, CWX = CTX + 2 * CK, CWY = CTY
 // neighbours of all but its end cells are its own registers.
 constexpr int CBY = 8, CNR = CWY / CBY, CNT = CWX * CBY, kChebBlocksPerSM = 2;
 static_assert(CWY % CBY == 0, "region rows must split evenly over the block rows");
-static_assert(CNT >= VTX * VTY, "the refinement tile needs a thread per cell");
 // Residual drop one FP32 inner cycle aims for (FP32 resolves about 1e-7; 1e-4 measured
 // 1.3% faster per step than 1e-5 and 2.4% faster than 1e-6 at 1024^2).
 constexpr double kChebDrop = 1e-4;
@@ -805,25 +804,51 @@ struct ChebTile {
 };
 
 // REFINE (and the START of a solve): stage x (the last ITER of the cycle has added the
-// correction) over a 32x8 tile and one-cell ring, r = rhs - (x - alpha A x) in FP64 at the
-// tile, |r|^2 and |b|^2; the next inner cycle starts from r: r_set = r, d_set = r / theta,
-// e_set = 0.
+// correction) over a CTX x CTY tile and its one-cell ring, r = rhs - (x - alpha A x) in
+// FP64 at the tile, |r|^2 and |b|^2; the next inner cycle starts from r: r_set = r,
+// d_set = r / theta, e_set = 0.  Every thread of the block takes up to kRefCells cells of
+// the tile, whose right-hand sides it loads together with its share of the ring, so a
+// tile is one round of independent loads and two barriers (the launch keeps the ITER
+// launches' block shape and occupancy).
+constexpr int RSX = CTX + 2, RSY = CTY + 2, kRefCells = (CTX * CTY + CNT - 1) / CNT;
+struct RefTileUV {  // the refinement tile: global requests, wrapped ones mapped back
+    const double* su;
+    const double* sv;
+    int i0, j0, Nx, Ny;
+    __device__ __forceinline__ int slot(int c, int r) const {
+        int lc = c - i0 + 1, lr = r - j0 + 1;
+        if (lc < 0) lc += Nx; else if (lc >= RSX) lc -= Nx;
+        if (lr < 0) lr += Ny; else if (lr >= RSY) lr -= Ny;
+        return lr * RSX + lc;
+    }
+    __device__ __forceinline__ double U(int c, int r) const { return su[slot(c, r)]; }
+    __device__ __forceinline__ double V(int c, int r) const { return sv[slot(c, r)]; }
+};
 template <bool START>
 __device__ void cheb_refine(const Params& P, double alpha, double theta, const ChebArgs& v, double* sm, double (&acc)[2]) {
     double* su = sm;
-    double* sv = sm + VSX * VSY;
+    double* sv = sm + RSX * RSY;
     const int tid = threadIdx.x + threadIdx.y * blockDim.x, nthr = blockDim.x * blockDim.y;
-    const int tx = tid % VTX, ty = tid / VTX;  // cell of the 32x8 tile (threads past it only load)
     const int Nx = P.g.Nx, Ny = P.g.Ny;
     const double mu = P.md.viscosity_fluid, ix2 = P.g.ihx * P.g.ihx, iy2 = P.g.ihy * P.g.ihy;
     const double cxx = 2.0 * mu * ix2, cyy = mu * iy2, cxx2 = mu * ix2, cyy2 = 2.0 * mu * iy2;
     const double cxy = mu * P.g.ihx * P.g.ihy;
-    const int ntx = (Nx + VTX - 1) / VTX, nt = ntx * ((Ny + VTY - 1) / VTY);
+    const int ntx = (Nx + CTX - 1) / CTX, nt = ntx * ((Ny + CTY - 1) / CTY);
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        const int i0 = (t % ntx) * VTX, j0 = (t / ntx) * VTY;
-        const int i = i0 + tx, j = j0 + ty;
-        for (int q = tid; q < VSX * VSY; q += nthr) {
-            const int gi = i0 + q % VSX - 1, gj = j0 + q / VSX - 1;
+        const int i0 = (t % ntx) * CTX, j0 = (t / ntx) * CTY;
+        double bu[kRefCells], bv[kRefCells];
+#pragma unroll
+        for (int m = 0; m < kRefCells; ++m) {
+            const int q = tid + m * nthr, i = i0 + q % CTX, j = j0 + q / CTX;
+            bu[m] = bv[m] = 0.0;
+            if (q < CTX * CTY && i < Nx && j < Ny) {
+                const size_t k = cidx(i, j, Nx);
+                bu[m] = v.rhs_u[k];
+                bv[m] = v.rhs_v[k];
+            }
+        }
+        for (int q = tid; q < RSX * RSY; q += nthr) {
+            const int gi = i0 + q % RSX - 1, gj = j0 + q / RSX - 1;
             const bool inx = gi >= 0 && gi < Nx, iny = gj >= 0 && gj < Ny;
             double hu = 0.0, hv = 0.0;
             if ((inx || P.g.px) && (iny || P.g.py)) {
@@ -835,25 +860,28 @@ __device__ void cheb_refine(const Params& P, double alpha, double theta, const C
             sv[q] = hv;
         }
         __syncthreads();
-        if (tid < VTX * VTY && i < Nx && j < Ny) {
+#pragma unroll
+        for (int m = 0; m < kRefCells; ++m) {
+            const int q = tid + m * nthr, tx = q % CTX, ty = q / CTX, i = i0 + tx, j = j0 + ty;
+            if (q >= CTX * CTY || i >= Nx || j >= Ny) continue;
             const size_t k = cidx(i, j, Nx);
-            const int sl = (ty + 1) * VSX + tx + 1;
+            const int sl = (ty + 1) * RSX + tx + 1;
             const double un = su[sl], vn = sv[sl];
             double au, av;
             if ((P.g.px || (i >= 1 && i <= Nx - 2)) && (P.g.py || (j >= 1 && j <= Ny - 2))) {
                 // free interior, constant viscosity: the compact stencil read from the tile
-                au = cxx * (su[sl + 1] - 2.0 * un + su[sl - 1]) + cyy * (su[sl + VSX] - 2.0 * un + su[sl - VSX]) +
-                     cxy * (sv[sl + VSX] - sv[sl + VSX - 1] - vn + sv[sl - 1]);
-                av = cxx2 * (sv[sl + 1] - 2.0 * vn + sv[sl - 1]) + cyy2 * (sv[sl + VSX] - 2.0 * vn + sv[sl - VSX]) +
-                     cxy * (su[sl + 1] - su[sl + 1 - VSX] - un + su[sl - VSX]);
+                au = cxx * (su[sl + 1] - 2.0 * un + su[sl - 1]) + cyy * (su[sl + RSX] - 2.0 * un + su[sl - RSX]) +
+                     cxy * (sv[sl + RSX] - sv[sl + RSX - 1] - vn + sv[sl - 1]);
+                av = cxx2 * (sv[sl + 1] - 2.0 * vn + sv[sl - 1]) + cyy2 * (sv[sl + RSX] - 2.0 * vn + sv[sl - RSX]) +
+                     cxy * (su[sl + 1] - su[sl + 1 - RSX] - un + su[sl - RSX]);
             } else {
-                visc_A<false>(P, MuConst{mu}, TileUV{su, sv, i0, j0, Nx, Ny}, i, j, au, av);
+                visc_A<false>(P, MuConst{mu}, RefTileUV{su, sv, i0, j0, Nx, Ny}, i, j, au, av);
             }
             const bool uf = u_fixed(P, i), vf = v_fixed(P, j);
-            const double r1 = uf ? 0.0 : v.rhs_u[k] - (un - alpha * au);
-            const double r2 = vf ? 0.0 : v.rhs_v[k] - (vn - alpha * av);
+            const double r1 = uf ? 0.0 : bu[m] - (un - alpha * au);
+            const double r2 = vf ? 0.0 : bv[m] - (vn - alpha * av);
             if (START) {  // |b|^2 of the row-eliminated system: Dirichlet rows hold their data
-                const double b1 = uf ? un : v.rhs_u[k], b2 = vf ? vn : v.rhs_v[k];
+                const double b1 = uf ? un : bu[m], b2 = vf ? vn : bv[m];
                 acc[1] += b1 * b1 + b2 * b2;
             }
             acc[0] += r1 * r1 + r2 * r2;
@@ -1055,7 +1083,7 @@ __device__ void cheb_iter(const Params& P, double alpha, double theta, double de
 // (dynamic shared memory: d double-buffered, e and r of special cells, the special-slot
 // list and the step coefficients)
 constexpr int kChebSmemBytes = 8 * CWX * CWY * 4 + CWX * CWY * 2 + 2 * CK * 4;
-static_assert(kChebSmemBytes >= 2 * VSX * VSY * 8, "the refinement tile shares the buffer");
+static_assert(kChebSmemBytes >= 2 * RSX * RSY * 8, "the refinement tile shares the buffer");
 static_assert(CWX * CWY <= 32767, "special slots are stored as short");
 
 template <bool START>
