@@ -1055,6 +1055,46 @@ __device__ void cheb_iter(const Params& P, double alpha, double theta, double de
             }
             __syncthreads();
         }
+        if (last) {
+            // end of the inner cycle: x += e (REFINE then restarts r, d, e).  e of the
+            // tile goes to the d buffer the last step read (free after its barrier), then
+            // the block adds it to x cell by cell, every thread's x loads issued together
+            // before its stores.
+            float* const fu = dbu[(CK & 1) ^ 1];
+            float* const fv = dbv[(CK & 1) ^ 1];
+#pragma unroll
+            for (int m = 0; m < CNR; ++m) {
+                const int ly = lyb + m, sl = ly * CWX + lx, gj = j0 + ly - CK;
+                if (lx < CK || lx >= CK + CTX || ly < CK || ly >= CK + CTY || gi >= Nx || gj >= Ny) continue;
+                float e1 = eu[m], e2 = ev[m], r1 = ru[m], r2 = rv[m];
+                if (skip & (1u << m)) { e1 = seu[sl]; e2 = sev[sl]; r1 = sru[sl]; r2 = srv[sl]; }
+                fu[sl] = e1;
+                fv[sl] = e2;
+                acc[0] += (double)r1 * r1 + (double)r2 * r2;
+            }
+            __syncthreads();
+            double xu[kRefCells], xv[kRefCells];
+#pragma unroll
+            for (int m = 0; m < kRefCells; ++m) {
+                const int q = tid + m * nthr, i = i0 + q % CTX, j = j0 + q / CTX;
+                xu[m] = xv[m] = 0.0;
+                if (q < CTX * CTY && i < Nx && j < Ny) {
+                    const size_t k = cidx(i, j, Nx);
+                    xu[m] = v.x_u[k];
+                    xv[m] = v.x_v[k];
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < kRefCells; ++m) {
+                const int q = tid + m * nthr, tx = q % CTX, ty = q / CTX, i = i0 + tx, j = j0 + ty;
+                if (q >= CTX * CTY || i >= Nx || j >= Ny) continue;
+                const int sl = (ty + CK) * CWX + tx + CK;
+                const size_t k = cidx(i, j, Nx);
+                v.x_u[k] = xu[m] + (double)fu[sl];
+                v.x_v[k] = xv[m] + (double)fv[sl];
+            }
+            continue;  // the next tile starts with a barrier
+        }
         // write the tile (special cells from shared memory; the latest d is in buffer CK & 1)
 #pragma unroll
         for (int m = 0; m < CNR; ++m) {
@@ -1066,14 +1106,9 @@ __device__ void cheb_iter(const Params& P, double alpha, double theta, double de
                 d1 = dbu[CK & 1][sl]; d2 = dbv[CK & 1][sl];
             }
             const size_t k = cidx(gi, gj, Nx);
-            if (last) {  // end of the inner cycle: x += e (REFINE then restarts r, d, e)
-                v.x_u[k] += (double)e1;
-                v.x_v[k] += (double)e2;
-            } else {
-                v.en_u[k] = e1; v.en_v[k] = e2;
-                v.rn_u[k] = r1; v.rn_v[k] = r2;
-                v.dn_u[k] = d1; v.dn_v[k] = d2;
-            }
+            v.en_u[k] = e1; v.en_v[k] = e2;
+            v.rn_u[k] = r1; v.rn_v[k] = r2;
+            v.dn_u[k] = d1; v.dn_v[k] = d2;
             acc[0] += (double)r1 * r1 + (double)r2 * r2;
         }
     }
