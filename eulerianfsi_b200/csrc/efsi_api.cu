@@ -786,7 +786,7 @@ void proj_solve(efsi_handle* h, int stage_slot, double reltol, const double* q0)
             [&](cudaStream_t s, int* io, cudaGraphConditionalHandle ch) {
                 // x transform (2 x 8 N B), y pass (2 x 8 N), x pass + update (3 x 8 N),
                 // residual (3 x 8 N)
-                site(h, EFSI_SITE_SPECTRAL, 8.0 * N * 9.0,
+                site(h, EFSI_SITE_SPECTRAL, 8.0 * N * 10.0,
                      [&] { proj_spectral_iter(P, h->pj, &d->cg_proj, &d->ps, h->slot[4], io, ch, s); });
             });
         return;
