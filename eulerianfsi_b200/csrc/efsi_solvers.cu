@@ -2022,7 +2022,8 @@ struct PredIn {
     }
 };
 
-__global__ void k_proj_rhs(Params P, PredIn in, const double* __restrict__ G, double* Up, double* Vp, double* rhs,
+// 64 registers at most: four blocks per SM
+__global__ void __launch_bounds__(256, 4) k_proj_rhs(Params P, PredIn in, const double* __restrict__ G, double* Up, double* Vp, double* rhs,
                            double* bw, int nullspace, ProjScal* ps, RedSlot rs, DevStatus* st) {
     __shared__ double sh[32 * 6];
     const int Nx = P.g.Nx, Ny = P.g.Ny;
@@ -2060,7 +2061,7 @@ __global__ void k_proj_rhs(Params P, PredIn in, const double* __restrict__ G, do
 void proj_rhs(const Params& P, const Projection& pj, bool compact_in, const double* u_in, const double* v_in,
               const double* G, ProjScal* ps, const RedSlot& rs, DevStatus* st, cudaStream_t s) {
     PredIn in{u_in, v_in, compact_in ? 1 : 0};
-    k_proj_rhs<<<persistent_grid(tiles2(P.g.Nx + 1, P.g.Ny + 1), P.nsm, 3), dim3(BX, BY), 0, s>>>(P, in, G, pj.Up, pj.Vp, pj.rhs, pj.b,
+    k_proj_rhs<<<persistent_grid(tiles2(P.g.Nx + 1, P.g.Ny + 1), P.nsm, 4), dim3(BX, BY), 0, s>>>(P, in, G, pj.Up, pj.Vp, pj.rhs, pj.b,
                                                                      pj.nullspace ? 1 : 0, ps, rs, st);
 }
 
@@ -2287,7 +2288,8 @@ __device__ __forceinline__ double q_grad_y(const Params& P, const double* x, dou
     return (q(j) - q(j - 1)) * P.g.ihy;
 }
 
-__global__ void k_proj_correct(Params P, MGLevel L, const double* __restrict__ x, const double* __restrict__ Up,
+// 64 registers at most: four blocks per SM
+__global__ void __launch_bounds__(256, 4) k_proj_correct(Params P, MGLevel L, const double* __restrict__ x, const double* __restrict__ Up,
                                const double* __restrict__ Vp, const double* __restrict__ G,
                                const double* __restrict__ rhs, double* q_out, double* U_out, double* V_out,
                                ProjScal* ps, double* stage_linf, RedSlot rmax, RedSlot rsum, DevStatus* st) {
@@ -2350,7 +2352,7 @@ void proj_finish(const Params& P, const Projection& pj, const double* G, double*
     const int nt = tiles2(L.nx, L.ny);
     dim3 b(BX, BY);
     k_proj_mean<<<persistent_grid(nt, P.nsm, 8), b, 0, s>>>(L, pj.x, ps, rs1, pj.nullspace ? 1 : 0);
-    k_proj_correct<<<persistent_grid(nt, P.nsm, 3), b, 0, s>>>(P, L, pj.x, pj.Up, pj.Vp, G, pj.rhs, q_out, U_out, V_out, ps, stage_linf, rs1,
+    k_proj_correct<<<persistent_grid(nt, P.nsm, 4), b, 0, s>>>(P, L, pj.x, pj.Up, pj.Vp, G, pj.rhs, q_out, U_out, V_out, ps, stage_linf, rs1,
                                    rs2, st);
 }
 

@@ -363,7 +363,8 @@ void proj_spectral_iter(const Params& P, const Projection& pj, CGScal* cg, const
     k_spec_b<<<gb, kSpecThreads, sp.smem_b, s>>>(sp, L.ax, L.ay, pj.z, pj.w, cg);
     k_spec_c<<<gc, kSpecThreads, sp.smem_c, s>>>(sp, pj.w, pj.x, cg, iters_out);
     const size_t nc = (size_t)L.nx * L.ny;
-    const int gr = (int)std::min<size_t>((nc + kSpecThreads - 1) / kSpecThreads, (size_t)std::max(P.nsm, 1) * 8);
+    // one persistent wave (two 512-thread blocks per SM at 64 registers)
+    const int gr = (int)std::min<size_t>((nc + kSpecThreads - 1) / kSpecThreads, (size_t)std::max(P.nsm, 1) * 2);
     k_spec_r<<<gr, kSpecThreads, 0, s>>>(L, sp.dx.logn, P.g.px, P.g.py, pj.b, pj.x, pj.r[0], ps, cg, rs, iters_out,
                                          cond);
 }
