@@ -847,7 +847,8 @@ __device__ bool sigma_log_product(double a, double d, double b, double& oxx, dou
 
 __device__ __forceinline__ double wall_u_at_xc(const SideD& s, int i) { return 0.5 * bval(s, i) + 0.5 * bval(s, i + 1); }
 
-__global__ void k_structure(Params P, const double* __restrict__ U, const double* __restrict__ V,
+// 64 registers at most: four blocks per SM
+__global__ void __launch_bounds__(256, 4) k_structure(Params P, const double* __restrict__ U, const double* __restrict__ V,
                             const double* __restrict__ phi, const double* __restrict__ sxx,
                             const double* __restrict__ syy, const double* __restrict__ sxy,
                             const double* __restrict__ G, double* Exx, double* Eyy, double* Exy, DevStatus* st) {
