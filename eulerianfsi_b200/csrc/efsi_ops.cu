@@ -573,8 +573,9 @@ __device__ __forceinline__ double ssd_y_in(const Params& P, const Cells& f, int 
     return dyy + dxy;
 }
 
+// 48 registers at most: five blocks per SM
 template <bool FULL>
-__global__ void k_momentum(Params P, double t, const double* __restrict__ U, const double* __restrict__ V,
+__global__ void __launch_bounds__(256, 5) k_momentum(Params P, double t, const double* __restrict__ U, const double* __restrict__ V,
                            Cells cells, const double* __restrict__ G, const double* __restrict__ kappa,
                            double* Fx, double* Fy) {
     const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
